@@ -1,0 +1,331 @@
+"""Throughput benchmark of the photon-transport hot path (LaunchOMP -> ComputePhoton) on B200.
+
+Workload (default): the 3-layer tissue with the top two boundaries triangulated height fields
+(256 x 256 vertices over 20 x 20 mm each, 2 x 130,050 triangles, A = 0.05 mm, lam = 2 mm), planar
+L2/L3 boundary and bottom, 50 rings of 0.1 mm and 200 time bins of 5 ps, roulette 1e-4 / 0.1;
+one step = one transport call of 1e7 photons. Synthetic input generated by xmcml_b200.scenes.
+
+  value : photons/s with the device image resident (xmc_run on a persistent context), device time
+          of every run from CUDA events on the library's stream (tally zeroing, kernel, read-back);
+          L2 is flushed between steps (256 MB write).
+  e2e   : photons/s through the reference-signature C-ABI xmc_launch_omp(InputInfo*, OutputInfo*,
+          MCG59*, int) with host buffers: every step uploads the device image (triangles, tree,
+          tables, detectors) from the caller's InputInfo (reference-layout BVH prebuilt once, as the
+          reference's launcher does), runs, reads the tallies back and adds them into the FP64
+          OutputInfo. Host wall clock around the call.
+  --impl reference : the reference's own OpenMP LaunchOMP (compiled from its sources into
+          oracle/_ref, -O3, all host threads) on a bounded sample of the same workload.
+Multi-GPU (torchrun): independent replicas on disjoint photon-id ranges (weak scaling); the only
+collectives are the barriers and the max-over-ranks of the timings.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "photons/s (3-layer, BVH mesh)"
+UNIT = "photons/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["heightfield", "planar"], default="heightfield")
+    p.add_argument("--photons", type=int, default=10_000_000)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_scene(workload, photons):
+    from xmcml_b200 import scenes
+    if workload == "heightfield":
+        return scenes.height_field_tissue(photons=photons), {
+            "workload": "heightfield-3layer-256x256-1e7", "surfaces": "2 height fields 256x256 (2x130050 tris) + 2 planes",
+            "rings": 50, "time_bins": "200 x 5 ps", "roulette": "1e-4 / 0.1", "grid": "100x100x100"}
+    return scenes.planar(photons=photons), {
+        "workload": "planar-3layer-1e6", "rings": 50, "grid": "100x100x100 over 10x10x5 mm", "roulette": "1e-4 / 0.1"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="xmc_clocks_", suffix=".csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_rate(xml, surf, seconds, threads, seed=777):
+    """The reference's LaunchOMP (oracle/_ref/libxmcml_ref_fast.so, -O3, all threads) on a bounded
+    sample of the workload; returns (photons/s, photons, seconds, threads)."""
+    from oracle import bind as OB
+    info = OB.ref_load_model(xml, surf, fast=True)
+    OB.ref(True).ref_generate_bvh(C.byref(info))  # prebuilt tree, outside the timed region
+    out = OB.ref_new_output(info, fast=True)
+    n = max(threads * 50, 500)
+    t0 = time.perf_counter()
+    OB.ref_launch(info, out, seed, threads, fast=True, n=n)
+    dt = time.perf_counter() - t0
+    rate = n / dt
+    n2 = int(max(threads * 100, min(rate * seconds, 5e7)))
+    out2 = OB.ref_new_output(info, fast=True)
+    t0 = time.perf_counter()
+    OB.ref_launch(info, out2, seed + 1, threads, fast=True, n=n2)
+    dt = time.perf_counter() - t0
+    return n2 / dt, n2, dt
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    d = tempfile.mkdtemp(prefix="xmc_bench_ref_")
+    sc, cfg = make_scene(args.workload, args.photons)
+    xml, surf = sc.write(d, "bench")
+    from oracle import bind as OB
+    if not OB.ref_available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libxmcml_ref_fast.so missing"}))
+        return
+    threads = os.cpu_count() or 1
+    info = OB.ref_load_model(xml, surf, fast=True)
+    OB.ref(True).ref_generate_bvh(C.byref(info))
+    # size one step at about 8 s of work from a probe run
+    out = OB.ref_new_output(info, fast=True)
+    n = max(threads * 50, 500)
+    t0 = time.perf_counter()
+    OB.ref_launch(info, out, 1, threads, fast=True, n=n)
+    rate0 = n / (time.perf_counter() - t0)
+    n_step = int(max(threads * 50, min(rate0 * 8.0, 5e7)))
+    for w in range(args.warmup):
+        OB.ref_launch(info, out, 100 + w, threads, fast=True, n=max(n_step // 4, threads * 10))
+    times = []
+    for k in range(args.steps):
+        out = OB.ref_new_output(info, fast=True)
+        t0 = time.perf_counter()
+        OB.ref_launch(info, out, 777 + k, threads, fast=True, n=n_step)
+        times.append(time.perf_counter() - t0)
+        OB.ref(True).ref_free_output(C.byref(out))
+    tot = sum(times)
+    value = n_step * args.steps / tot
+    cfg = dict(cfg)
+    cfg["parallelism"] = f"OpenMP x{threads} (host CPU)"
+    cfg["semantics"] = "reference: weight cut at MinWeight 1e-4, Area kill (no roulette in the reference)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{n_step} photons per step of the same workload, LaunchOMP with {threads} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def roofline(led, kernel_ms, clocks, n_photons):
+    """Issue-bound roofline of the transport kernel from the per-step cost model (48 FP32 flop,
+    6 MUFU and ~45 INT32 ops of Philox per walk iteration, plus 16 flop per BVH node test and
+    30 flop per triangle test), against the nominal SIMT peak 148 SMs x 128 lanes x SM clock."""
+    steps = led["steps"]
+    nodes = led["n_node_visits"]
+    tris = led["n_triangle_tests"]
+    ops = steps * (48 + 45) + nodes * 16 + tris * 30
+    t = kernel_ms / 1e3
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    peak_ops = 148 * 128 * sm_mhz * 1e6
+    achieved = ops / t
+    mufu = steps * 6 / t
+    mufu_peak = 148 * 16 * sm_mhz * 1e6
+    return {"bound": "issue", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TOP/s",
+            "frac": achieved / peak_ops, "traffic": None,
+            "model": {"ops_per_step": (48 + 45), "node_tests_per_step": nodes / max(steps, 1),
+                      "triangle_tests_per_step": tris / max(steps, 1), "steps_per_photon": steps / max(n_photons, 1),
+                      "mufu_frac": mufu / mufu_peak,
+                      "peak_source": "nominal 148 SMs x 128 FP32/INT32 lanes x median sampled SM clock (MEASURED_PEAKS.json "
+                                     "has no SIMT figure; the walk is not HBM- or tensor-bound)"}}
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    from xmcml_b200 import api, _lib
+    from xmcml_b200 import structs as S
+    d = tempfile.mkdtemp(prefix=f"xmc_bench_{rank}_")
+    sc, cfg = make_scene(args.workload, args.photons)
+    xml, surf = sc.write(d, "bench")
+    m = api.Model(xml, surf)
+    N = args.photons
+    t = api.Transport(m, roulette=True, device=local)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+
+    base = rank * (args.warmup + args.steps) * N  # disjoint photon ids per rank and step
+    for w in range(args.warmup):
+        t.run(N, seed=777, first_photon=base + w * N)
+    barrier()
+    leds = []
+    with ClockSampler(local) as clk:
+        barrier()
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            leds.append(t.run(N, seed=777, first_photon=base + (args.warmup + k) * N))
+        barrier()
+    clocks = clk.summary()
+    dev_ms = sum(l["total_ms"] for l in leds)
+    ker_ms = sum(l["kernel_ms"] for l in leds)
+    if dist is not None:
+        tt = torch.tensor([dev_ms, ker_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms, ker_ms = tt.tolist()
+    value = world * args.steps * N / (dev_ms / 1e3)
+    tal = t.tallies()
+    last = leds[-1]
+
+    # ---- e2e through the reference-signature C-ABI with host buffers ----
+    lib = _lib.load()
+    tree = lib.xmc_generate_bvh_tree(m.info.surface, m.info.numberOfSurfaces)  # prebuilt once, like the reference launcher
+    m.info.bvhTree = tree
+    m.info.numberOfPhotons = N
+    probe = api.Transport(m, roulette=False, device=local)
+    pled = probe.run(1000, seed=1)
+    probe.close()
+    h2d = pled["h2d_bytes"]
+    out = api.Output(m)
+    rng = api.mcg59_init(777 + rank, 0, 1)
+    api.launch_omp(m, out, rng, 0)  # warm
+    barrier()
+    e2e_t = []
+    for k in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        api.launch_omp(m, out, rng, 0)
+        e2e_t.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = sum(e2e_t)
+    if dist is not None:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = tt.item()
+    e2e_value = world * args.e2e_steps * N / e2e_s
+    grid = out.info.gridSize
+    D = out.info.numberOfDetectors
+    T = m.info.timeScaleSize
+    d2h = 8 * grid + 32 * D + 32 * D * T + 8 * 32 + 16
+    m.info.bvhTree = None
+    lib.xmc_free_bvh_tree(tree)
+
+    rl = roofline(last, last["kernel_ms"], clocks, N)
+    prof = os.path.join(ROOT, "profiles", f"transport_kernel_{args.workload}_dram.json")
+    if os.path.exists(prof):
+        try:
+            pj = json.load(open(prof))
+            rl["traffic"] = pj.get("dram_bytes_per_launch")
+            rl["traffic_note"] = pj.get("note")
+        except Exception:
+            pass
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import bind as OB
+            if OB.ref_available(fast=True):
+                rate, n_cpu, secs = cpu_reference_rate(xml, surf, args.cpu_seconds, os.cpu_count() or 1)
+                cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference",
+                       "sample": f"{n_cpu} photons of the same workload through the reference's LaunchOMP "
+                                 f"({secs:.1f} s, -O3, reference semantics: weight cut, no roulette)"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    cfg = dict(cfg)
+    cfg["photons_per_step"] = N
+    cfg["parallelism"] = f"replicas x{world} (disjoint photon ids)"
+    cfg["l2"] = "flushed between timed steps (256 MB write)"
+    cfg["launch"] = {"block": t.opts.block_size or 256}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": cfg, "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "via": "xmc_launch_omp (LaunchOMP signature), host InputInfo/OutputInfo"},
+            "gpu_launches": args.steps, "roofline": rl, "cpu_baseline": cpu,
+            "kernel_ms_per_step": ker_ms / args.steps,
+            "walk": {"steps_per_photon": last["steps"] / N, "detected_fraction": last["n_detected"] / N,
+                     "fp64_retests_per_step": last["n_fp64_retests"] / max(last["steps"], 1),
+                     "escaped_top": last["escaped_top"], "absorbed": last["absorbed"]}}
+    t.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,356 @@
+/*
+ * xmcml_b200 — C-ABI of the B200 photon-transport library.
+ *
+ * The library replaces the node driver of xMCML (the OpenMP `LaunchOMP` call and the
+ * `ComputePhoton` walk below it) with one persistent CUDA kernel per call on an sm_100a GPU.
+ *
+ * Part 1 declares the reference's own data structures with the reference's field order, types
+ * and struct tags, so a caller built against the reference headers passes the same objects:
+ *   base/xmcml/xmcml/mcml_types.h:1-41           (double3, int3, byte3, Area, Surface)
+ *   base/xmcml/xmcml/mcml_intersection.h:12-57   (IntersectionInfo, Triangle, AABB, BVHNode, BVHTree)
+ *   base/xmcml/xmcml/mcml_kernel_types.h:7-124   (TimeInfo ... PhotonTrajectory, MAX_LAYERS)
+ *   base/xmcml/xmcml/mcml_mcg59.h:6-10           (MCG59)
+ * The layouts are checked field by field against the reference headers by the test suite
+ * (xmc_layout_offsets below).
+ *
+ * Part 2 declares the entry points. Every function returns an xmc_status (0 = success) unless
+ * it mirrors a reference function whose return type it keeps; xmc_last_error() gives the text of
+ * the last failure on the calling thread.
+ */
+#ifndef XMCML_B200_H
+#define XMCML_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- Part 1: reference layouts */
+
+#define MAX_LAYERS 8
+#define MAX_TRAJECTORY_SIZE 20480
+
+typedef unsigned char byte;
+typedef unsigned int uint;
+typedef unsigned long long int uint64;
+
+typedef union __double3 {
+    struct { double x, y, z; };
+    struct { double cell[3]; };
+} double3;
+
+typedef union __int3 {
+    struct { int x, y, z; };
+    struct { int cell[3]; };
+} int3;
+
+typedef union __byte3 {
+    struct { byte x, y, z; };
+    struct { byte cell[3]; };
+} byte3;
+
+typedef struct __Area {
+    double3 corner;
+    double3 length;
+    int3 partitionNumber;
+} Area;
+
+typedef struct __Surface {
+    double3* vertices;
+    int numberOfVertices;
+    int3* triangles;
+    int numberOfTriangles;
+} Surface;
+
+typedef struct __IntersectionInfo {
+    double3 normal;
+    double distance;
+    int surfaceId;
+    int isFindIntersection;
+} IntersectionInfo;
+
+typedef struct __Triangle {
+    int surfId;
+    int trIndex;
+} Triangle;
+
+typedef struct __AABB {
+    double3 Ver1;
+    double3 Ver2;
+} AABB;
+
+/* The reference gives BVHNode and BVHTree C++ constructors; the layout is the same. */
+typedef struct __BVHNode {
+    AABB Box;
+    int rightNode;
+    int leftNode;
+    int offset;
+    int numOfTriangles;
+} BVHNode;
+
+typedef struct __BVHTree {
+    BVHNode* nodes;
+    int numOfNodes;
+    int root;
+    Triangle* triangles;
+    int numOfTriangles;
+} BVHTree;
+
+typedef struct __TimeInfo {
+    double timeStart;
+    double timeFinish;
+    uint64 numberOfPhotons;
+    double weight;
+    double targetWeight;
+} TimeInfo;
+
+typedef struct __CubeDetector {
+    double3 center;
+    double3 length;
+    bool filterLayers[MAX_LAYERS];
+    double targetAngle;
+} CubeDetector;
+
+typedef struct __RingDetector {
+    double3 center;
+    double smallRadius;
+    double bigRadius;
+    bool filterLayers[MAX_LAYERS];
+    double targetAngle;
+} RingDetector;
+
+typedef struct __DetectorInfo {
+    uint64 numberOfPhotons;
+    uint64* trajectory;
+    int trajectorySize;
+    TimeInfo* timeScale;
+    int timeScaleSize;
+    double targetWeight;
+    double weight;
+} DetectorInfo;
+
+typedef struct __WeightIntegralTable {
+    double anisotropy;
+    int numberOfElements;
+    double* elements;
+} WeightIntegralTable;
+
+typedef struct __LayerInfo {
+    double refractiveIndex;
+    double absorptionCoefficient;
+    double scatteringCoefficient;
+    double anisotropy;
+    int* surfaceId;
+    int numberOfSurfaces;
+} LayerInfo;
+
+typedef struct __InputInfo {
+    uint64 numberOfPhotons;
+    Area* area;
+    LayerInfo* layerInfo;
+    int numberOfLayers;
+    Surface* surface;
+    int numberOfSurfaces;
+    CubeDetector* cubeDetector;
+    int numberOfCubeDetectors;
+    RingDetector* ringDetector;
+    int numberOfRingDetectors;
+    double minWeight;
+    BVHTree* bvhTree;
+    double timeStart;
+    double timeFinish;
+    int timeScaleSize;
+    double3 startPosition;
+    double3 startDirection;
+    byte useBiasing;
+    uint weightIntegralPrecision;
+    uint weightTablePrecision;
+    double attractiveFactor;
+    WeightIntegralTable* weightTable;
+    int numberOfWeightTables;
+    double3 targetPoint;
+    unsigned char targetRangeLayers[MAX_LAYERS];
+} InputInfo;
+
+typedef struct __OutputInfo {
+    uint64 numberOfPhotons;
+    double specularReflectance;
+    double* absorption;
+    double* scattering;
+    int gridSize;
+    DetectorInfo* detectorInfo;
+    int numberOfDetectors;
+} OutputInfo;
+
+typedef struct __MCG59 {
+    uint64 value;
+    uint64 offset;
+} MCG59;
+
+/* ---------------------------------------------------------------- Part 2: entry points */
+
+typedef enum xmc_status {
+    XMC_OK = 0,
+    XMC_ERR_INVALID_INPUT = 1,   /* a field of InputInfo/OutputInfo is missing or inconsistent */
+    XMC_ERR_RANGE = 2,           /* a size is outside what the library supports (e.g. partition > 256) */
+    XMC_ERR_DEVICE = 3,          /* a CUDA call failed; the text names it */
+    XMC_ERR_BUDGET = 4,          /* a photon hit the per-photon step budget (it was terminated) */
+    XMC_ERR_CANCELLED = 5,       /* xmc_cancel() stopped the run; tallies hold the photons done */
+    XMC_ERR_IO = 6,              /* a file could not be read or written */
+    XMC_ERR_UNSUPPORTED = 7      /* a reference feature the GPU path does not provide (biasing) */
+} xmc_status;
+
+/* Option flags (xmc_options.flags). */
+#define XMC_ROULETTE        (1u << 0)  /* Russian roulette at minWeight instead of killing the photon */
+#define XMC_NO_AREA_KILL    (1u << 1)  /* photons leaving Area keep walking; their absorption goes to
+                                          the ledger's absorbed_outside term                         */
+#define XMC_SCATTERING_MAP  (1u << 2)  /* tally the z-plane crossing map OutputInfo.scattering         */
+#define XMC_DETECTOR_TRAJ   (1u << 3)  /* tally per-detector trajectory maps DetectorInfo.trajectory   */
+#define XMC_LARGE_GRID      (1u << 4)  /* accept Area partitions above 256 per axis (the reference wraps
+                                          voxel indices at 256; this library indexes them in full)    */
+
+typedef struct xmc_options {
+    uint32_t struct_size;          /* sizeof(xmc_options); 0 selects all defaults                */
+    uint32_t flags;                /* XMC_* flags above                                           */
+    double   roulette_chance;      /* survival probability of roulette (default 0.1)             */
+    double   beam_radius;          /* uniform-disk beam radius in mm around startPosition (0 = pencil) */
+    uint64_t max_steps_per_photon; /* step budget per photon (0 = 10,000,000)                    */
+    int32_t  device;               /* CUDA device ordinal (default 0)                            */
+    int32_t  block_size;           /* threads per block (0 = autotuned / default 256)             */
+    int32_t  blocks_per_sm;        /* resident blocks per SM (0 = occupancy maximum)              */
+    int32_t  photons_per_chunk;    /* photon ids a warp claims at a time (0 = 256)                */
+    int32_t  smem_nodes;           /* BVH nodes staged in shared memory (-1 = none, 0 = auto)      */
+    int32_t  reserved[7];
+} xmc_options;
+
+/* Energy ledger of one or more runs: every photon's start weight 1 is split exactly into these
+ * terms. The *_fx fields are the raw 64-bit fixed-point sums (weight * 2^31); the double fields
+ * are the same sums divided by the number of photons. specular + absorbed + absorbed_outside +
+ * escaped_top + escaped_bottom + lost_area + lost_cut + lost_glass + lost_budget + lost_invalid
+ * + roulette_killed - roulette_gained == 1 holds exactly in the fixed-point sums. */
+typedef struct xmc_ledger {
+    uint64_t photons_launched;
+    uint64_t photons_terminated;
+    uint64_t steps;                /* walk-loop iterations                                      */
+    uint64_t n_escaped_top, n_escaped_bottom, n_area, n_cut, n_roulette, n_glass, n_budget, n_invalid;
+    uint64_t n_detected;           /* photons that scored in a detector                        */
+    uint64_t n_fp64_retests;       /* ray-triangle tests redone in FP64 in an edge band          */
+    uint64_t n_node_visits;        /* BVH nodes visited by all ray queries                      */
+    uint64_t n_triangle_tests;     /* ray-triangle tests                                        */
+    uint64_t specular_fx, absorbed_fx, absorbed_outside_fx, escaped_top_fx, escaped_bottom_fx,
+             lost_area_fx, lost_cut_fx, lost_glass_fx, lost_budget_fx, lost_invalid_fx,
+             roulette_killed_fx, roulette_gained_fx;
+    double specular, absorbed, absorbed_outside, escaped_top, escaped_bottom, lost_area, lost_cut,
+           lost_glass, lost_budget, lost_invalid, roulette_killed, roulette_gained;
+    double kernel_ms;              /* device time of the transport kernel(s), CUDA events       */
+    double total_ms;               /* device time of the whole run incl. zeroing and read-back  */
+    uint64_t h2d_bytes;            /* bytes copied host->device for the context's device image  */
+    uint64_t d2h_bytes;            /* bytes copied device->host by this run                     */
+} xmc_ledger;
+
+typedef struct xmc_context xmc_context;
+
+/* Library version as 10000*major + 100*minor + patch. */
+int xmc_version(void);
+
+/* Text of the last error on this thread ("" if none). */
+const char* xmc_last_error(void);
+
+/* Fill *opt with defaults (sets struct_size). */
+void xmc_default_options(xmc_options* opt);
+
+/* Build a device image of `input` (layers, triangles, BVH, detectors, time bins, Area) on the
+ * GPU. Uses input->bvhTree when it is set (the reference's GenerateBVHTree output, as the
+ * reference's launchers prebuild it: base/xmcml/xmcmlLauncher/launcher_mpi.cpp:396), else builds
+ * a BVH itself. Does not retain any pointer into `input`. */
+int xmc_create(const InputInfo* input, const xmc_options* opt, xmc_context** out_ctx);
+
+/* Run photons [first_photon_id, first_photon_id + n_photons) with counter-RNG key `seed` and
+ * ADD the tallies to `output` (reference semantics: LaunchOMP accumulates,
+ * base/xmcml/xmcmlLauncher/launcher_omp.cpp:146-154), setting output->specularReflectance.
+ * `output` may be NULL (tallies stay on the device, see xmc_read_tallies); `ledger` may be NULL.
+ * Returns XMC_ERR_BUDGET if any photon hit the step budget (tallies are still valid). */
+int xmc_run(xmc_context* ctx, uint64_t seed, uint64_t first_photon_id, uint64_t n_photons,
+            OutputInfo* output, xmc_ledger* ledger);
+
+/* Raw 64-bit fixed-point device tallies of the last xmc_run, copied to host arrays (any may be
+ * NULL): absorption[gridSize], detector weight/count/targetWeight/weight^2 [numberOfDetectors],
+ * time bins weight/count/targetWeight/weight^2 [numberOfDetectors * timeScaleSize]. */
+int xmc_read_tallies(xmc_context* ctx, uint64_t* absorption, uint64_t* det_weight,
+                     uint64_t* det_count, uint64_t* det_target, uint64_t* det_weight2,
+                     uint64_t* time_weight, uint64_t* time_count, uint64_t* time_target,
+                     uint64_t* time_weight2);
+
+/* Ask a running xmc_run on another thread to stop after the photons in flight. */
+int xmc_cancel(xmc_context* ctx);
+
+int xmc_destroy(xmc_context* ctx);
+
+/* One call = create + run + destroy. */
+int xmc_launch(const InputInfo* input, OutputInfo* output, uint64_t seed,
+               uint64_t first_photon_id, const xmc_options* opt, xmc_ledger* ledger);
+
+/* Replaces LaunchOMP(InputInfo*, OutputInfo*, MCG59*, int)
+ * (base/xmcml/xmcmlLauncher/launcher_omp.h:10, launcher_omp.cpp:123-163): runs
+ * input->numberOfPhotons photons on the GPU and adds the tallies to `output` (output->
+ * numberOfPhotons is left to the caller, as the reference does). The counter-RNG key is
+ * randomGenerator[0].value and the photons are ids 0..numberOfPhotons-1; afterwards
+ * randomGenerator[0] is advanced by one MCG59 step, so consecutive calls (the reference's backup
+ * portions, launcher_mpi.cpp:357-380) use fresh keys. numThreads is ignored. Default options
+ * (reference semantics: weight cut at minWeight, photons killed outside Area). Returns 0 on
+ * success; on failure it prints xmc_last_error() to stderr and returns the status. */
+int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* randomGenerator, int numThreads);
+
+/* Replaces InitOutput / FreeOutput (base/xmcml/xmcmlLauncher/launcher_omp.cpp:10-58, 76-104):
+ * allocates and zeroes the tally arrays of `output` for `input`. */
+void xmc_init_output(InputInfo* input, OutputInfo* output);
+void xmc_free_output(OutputInfo* output);
+
+/* Replaces ParseInputFile / ParseSurfaceFile (base/xmcml/xmcmlLauncher/parser.cpp:18-514,
+ * 583-611): reads the reference's XML model and binary .surface file into `input`.
+ * Return true on success, like the reference. */
+bool xmc_parse_input_file(const char* fileName, InputInfo* input);
+bool xmc_parse_surface_file(const char* fileName, InputInfo* input);
+void xmc_free_input(InputInfo* input);
+
+/* Replaces WriteOutputToFile (base/xmcml/xmcmlLauncher/writer.cpp:431-471): writes the
+ * sectioned binary .mcml.out. Returns true on success, like the reference. */
+bool xmc_write_output_file(InputInfo* input, OutputInfo* output, const char* fileName);
+
+/* Replaces GenerateBVHTree (base/xmcml/xmcml/mcml_intersection.cpp:316-344): builds a binned-SAH
+ * BVH over all triangles of `surfaces` in the reference's BVHTree layout (FP64 boxes, leaves as
+ * (surfId, trIndex) runs), for callers that prebuild input->bvhTree once (launcher_mpi.cpp:396).
+ * Returns NULL on invalid input (see xmc_last_error). Free with xmc_free_bvh_tree. */
+BVHTree* xmc_generate_bvh_tree(const Surface* surfaces, int numberOfSurfaces);
+void xmc_free_bvh_tree(BVHTree* tree);
+
+/* Replaces ComputeSpecularReflectance (base/xmcml/xmcml/mcml_kernel.cpp:16-37). */
+double xmc_specular_reflectance(const LayerInfo* layer);
+
+/* Counter RNG used by the kernel: Philox4x32-10 (Salmon et al., SC'11) of counter
+ * (ctr[0..3]) and key (key[0..1]); host implementation for tests and tools. */
+void xmc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Byte offsets of the Part 1 struct fields in a fixed order (see layout.cpp); returns count. */
+int xmc_layout_offsets(int64_t* out, int max_count);
+
+/* Self test of the kernel's ray query compiled for the host: for each ray (ox,oy,oz,dx,dy,dz in
+ * rays[6*i]) the nearest hit with tmin <= t <= tmax over the device image of `input` (distance,
+ * surface id or -1, unit normal or NULL). Used by the CPU test suite. */
+int xmc_debug_nearest(const InputInfo* input, int n_rays, const float* rays, float tmin, float tmax,
+                      float* t_out, int* surf_out, float* normal_out);
+
+/* Run the photon kernel's device-side self test: `n` Philox blocks for the given key written to
+ * out[4*n] (device path), for comparing with xmc_philox4x32_10. */
+int xmc_device_philox(uint64_t seed, uint64_t photon_id, uint32_t n, uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XMCML_B200_H */

@@ -1,0 +1,261 @@
+"""Parity of the CUDA transport kernel (through the C-ABI) with the FP64 oracle.
+
+Both draw the same random numbers (Philox4x32-10 keyed by seed and photon id, one block of four
+uniforms per walk iteration), so most photons follow the same path in FP32 and in FP64 and the
+tallies agree far inside the Monte Carlo error; the checks are
+  * exact: launched == terminated == N, the per-cause counts add up, and the fixed-point energy
+    ledger closes exactly (specular + absorbed + escaped + losses + roulette killed - gained == N);
+  * statistical (3 sigma contract): every ring / time-bin / ledger total within 3 combined
+    standard errors of the oracle (variances from per-photon sums of squares), and within 0.5
+    combined standard errors for the totals (the paths are shared);
+  * bit-reproducibility of the integer tallies across launch shapes.
+"""
+import ctypes as C
+import os
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from oracle import bind as B
+from xmcml_b200 import _lib, api, scenes
+from xmcml_b200 import structs as S
+
+from helpers import WEIGHT_SCALE, ledger_identity_fx, oracle_opts_for, rich_planar, sum_var, zscores
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_pair(tmp_path, sc, n, seed=777, roulette=False, area_kill=True, beam_radius=0.0, stem="s", **kw):
+    xml, surf = sc.write(str(tmp_path), stem)
+    m = api.Model(xml, surf)
+    t = api.Transport(m, roulette=roulette, area_kill=area_kill, beam_radius=beam_radius, **kw)
+    led = t.run(n, seed=seed)
+    tal = t.tallies()
+    out = api.Output(m)
+    oled, dw2, tw2 = B.oracle_run(m.info, out.info, oracle_opts_for(roulette, area_kill, beam_radius), seed=seed, n=n)
+    t.close()
+    return m, led, tal, out, oled, dw2, tw2
+
+
+def _check_exact(led, n):
+    assert led["photons_launched"] == n
+    assert led["photons_terminated"] == n
+    causes = ["n_escaped_top", "n_escaped_bottom", "n_area", "n_cut", "n_roulette", "n_glass", "n_budget", "n_invalid"]
+    assert sum(led[c] for c in causes) == n
+    assert ledger_identity_fx(led) == n * 2 ** 31
+
+
+def _check_rings(tal, out, dw2, n, label):
+    g = tal["det_weight"].astype(float) / WEIGHT_SCALE
+    g2 = tal["det_weight2"].astype(float) / WEIGHT_SCALE
+    o = out.detector_weights()
+    z = zscores(g, o, sum_var(g, g2, n), sum_var(o, dw2, n))
+    print(f"{label}: rings max|z| {np.max(np.abs(z)):.3f}, sum gpu {g.sum():.2f} oracle {o.sum():.2f}")
+    assert np.all(np.abs(z) < 3.0)
+    zt = zscores(g.sum(), o.sum(), sum_var(g.sum(), g2.sum(), n), sum_var(o.sum(), dw2.sum(), n))
+    assert abs(zt) < 0.5
+    # detected photon counts (binomial)
+    c = tal["det_count"].astype(float)
+    oc = out.detector_counts().astype(float)
+    zc = zscores(c, oc, c * (1 - c / n), oc * (1 - oc / n))
+    assert np.all(np.abs(zc) < 3.0)
+    return z
+
+
+def _check_ledger_terms(led, oled, n, label):
+    """Totals of the energy ledger (each photon scores at most its start weight in one term)."""
+    for k in ["escaped_top", "escaped_bottom", "lost_area", "lost_cut", "roulette_killed"]:
+        g = led[k + "_fx"] / WEIGHT_SCALE
+        o = oled[k]
+        # binomial-type variance bound: a term of total T from n photons, each <= 1: var <= T
+        z = (g - o) / np.sqrt(max(g + o, 1e-12))
+        print(f"{label}: {k} gpu {g / n:.6f} oracle {o / n:.6f} z {z:.3f}")
+        assert abs(z) < 3.0
+    ga = led["absorbed_fx"] / WEIGHT_SCALE + led["absorbed_outside_fx"] / WEIGHT_SCALE
+    oa = oled["absorbed"] + oled["absorbed_outside"]
+    assert abs(ga - oa) / n < 5e-3
+
+
+def test_c1_reference_semantics(tmp_path):
+    """3-layer planar config: weight cut at minWeight, Area kill (the reference's own semantics)."""
+    n = 200_000
+    m, led, tal, out, oled, dw2, tw2 = _run_pair(tmp_path, scenes.planar(photons=n), n)
+    _check_exact(led, n)
+    assert oled["launched"] == oled["terminated"] == n
+    _check_rings(tal, out, dw2, n, "c1")
+    _check_ledger_terms(led, oled, n, "c1")
+    # absorption per depth slab and per radial shell of voxels
+    ga = tal["absorption"].astype(float).reshape(100, 100, 100) / WEIGHT_SCALE
+    oa = out.absorption.reshape(100, 100, 100)
+    for axis_sum in [(0, 1), (1, 2)]:
+        gs, os_ = ga.sum(axis=axis_sum), oa.sum(axis=axis_sum)
+        rel = np.abs(gs - os_) / np.maximum(os_, 1e-9)
+        big = os_ > 0.02 * os_.max()
+        print("c1 absorption profile max rel diff", rel[big].max())
+        assert rel[big].max() < 0.02
+    assert led["steps"] == pytest.approx(oled["steps"], rel=0.01)
+
+
+def test_c1_roulette_no_area_kill(tmp_path):
+    """BASELINE semantics: roulette 1e-4 / 0.1 and no Area kill; R + T + A + losses == 1 exactly."""
+    n = 100_000
+    m, led, tal, out, oled, dw2, tw2 = _run_pair(tmp_path, scenes.planar(photons=n), n, roulette=True, area_kill=False)
+    _check_exact(led, n)
+    assert led["n_area"] == 0 and led["n_roulette"] > 0
+    total = sum(led[k] for k in S.LEDGER_TERMS if k != "roulette_gained") - led["roulette_gained"]
+    assert abs(total - 1.0) < 1e-9
+    _check_rings(tal, out, dw2, n, "c1r")
+    _check_ledger_terms(led, oled, n, "c1r")
+
+
+def test_height_field_rings_and_time_bins(tmp_path):
+    n = 100_000
+    sc = scenes.height_field_tissue(photons=n, grid=96, time_bins=40)
+    m, led, tal, out, oled, dw2, tw2 = _run_pair(tmp_path, sc, n, roulette=True)
+    _check_exact(led, n)
+    assert led["n_invalid"] == 0
+    _check_rings(tal, out, dw2, n, "hf")
+    _check_ledger_terms(led, oled, n, "hf")
+    g = tal["time_weight"].astype(float) / WEIGHT_SCALE
+    g2 = tal["time_weight2"].astype(float) / WEIGHT_SCALE
+    o = out.time_weights()
+    z = zscores(g, o, sum_var(g, g2, n), sum_var(o, tw2, n))
+    print("hf time bins max|z|", np.max(np.abs(z)))
+    assert np.all(np.abs(z) < 3.0)
+
+
+def test_glass_cubes_filters_targets_beam(tmp_path):
+    n = 100_000
+    sc = rich_planar(n)
+    m, led, tal, out, oled, dw2, tw2 = _run_pair(tmp_path, sc, n, roulette=True, beam_radius=0.3)
+    _check_exact(led, n)
+    _check_rings(tal, out, dw2, n, "rich")
+    g = tal["det_target"].astype(float) / WEIGHT_SCALE
+    o = out.detector_target_weights()
+    gw = tal["det_weight"].astype(float) / WEIGHT_SCALE
+    rel = np.abs(g - o) / np.maximum(np.abs(o), 1e-9)
+    print("rich target weights", g, o)
+    assert np.all((rel < 0.03) | (np.abs(g - o) < 0.01 * gw.sum() / len(gw)))
+    g = tal["time_weight"].astype(float) / WEIGHT_SCALE
+    z = zscores(g, out.time_weights(), sum_var(g, tal["time_weight2"].astype(float) / WEIGHT_SCALE, n),
+                sum_var(out.time_weights(), tw2, n))
+    assert np.all(np.abs(z) < 3.0)
+
+
+def test_bit_reproducible_across_launch_shapes(tmp_path):
+    n = 50_000
+    xml, surf = scenes.height_field_tissue(photons=n, grid=64, time_bins=20).write(str(tmp_path), "rep")
+    m = api.Model(xml, surf)
+    res = []
+    for kw in [dict(), dict(block_size=128, blocks_per_sm=1, photons_per_chunk=32), dict(block_size=512, smem_nodes=-1)]:
+        t = api.Transport(m, roulette=True, **kw)
+        led = t.run(n, seed=99)
+        res.append((t.tallies(), led))
+        t.close()
+    for tal, led in res[1:]:
+        for k in tal:
+            assert np.array_equal(tal[k], res[0][0][k]), k
+        for k in S.LEDGER_TERMS:
+            assert led[k + "_fx"] == res[0][1][k + "_fx"]
+
+
+def test_split_runs_add_up(tmp_path):
+    """Photons are identified by id: running [0, n) in two calls gives the same integer tallies."""
+    n = 40_000
+    xml, surf = scenes.planar(photons=n).write(str(tmp_path), "split")
+    m = api.Model(xml, surf)
+    t = api.Transport(m, roulette=True)
+    t.run(n, seed=5)
+    whole = t.tallies()
+    t.run(n // 4, seed=5, first_photon=0)
+    a = t.tallies()
+    t.run(n - n // 4, seed=5, first_photon=n // 4)
+    b = t.tallies()
+    for k in whole:
+        assert np.array_equal(whole[k], a[k] + b[k]), k
+    t.close()
+
+
+def test_launch_omp_shim_accumulates(tmp_path):
+    n = 20_000
+    xml, surf = scenes.planar(photons=n).write(str(tmp_path), "omp")
+    m = api.Model(xml, surf)
+    out = api.Output(m)
+    rng = api.mcg59_init(777, 0, 1)
+    v0 = rng.value
+    api.launch_omp(m, out, rng, 8)
+    w1 = out.detector_weights().sum()
+    assert out.info.specularReflectance == pytest.approx(0.0277777777777, rel=1e-9)
+    assert out.info.numberOfPhotons == 0  # left to the caller, as the reference's LaunchOMP does
+    assert rng.value != v0
+    api.launch_omp(m, out, rng, 8)
+    w2 = out.detector_weights().sum()
+    assert 1.8 * w1 < w2 < 2.2 * w1
+    assert out.detector_counts().sum() > 0 and out.absorption.sum() > 0
+    p = str(tmp_path / "r.mcml.out")
+    out.write(p)
+    assert os.path.getsize(p) > out.info.gridSize * 8
+
+
+def test_device_philox_matches_host():
+    lib = _lib.load()
+    n = 1000
+    dev = (C.c_uint32 * (4 * n))()
+    _lib.check(lib.xmc_device_philox(0x123456789ABCDEF, 77, n, dev))
+    host = (C.c_uint32 * 4)()
+    for i in [0, 1, 17, 999]:
+        ctr = (C.c_uint32 * 4)(77, 0, i, 0)
+        key = (C.c_uint32 * 2)(0x89ABCDEF, 0x1234567)
+        lib.xmc_philox4x32_10(ctr, key, host)
+        assert list(host) == list(dev[4 * i:4 * i + 4])
+
+
+def test_step_budget_terminates_and_reports(tmp_path):
+    n = 10_000
+    xml, surf = scenes.planar(photons=n).write(str(tmp_path), "budget")
+    m = api.Model(xml, surf)
+    t = api.Transport(m, max_steps=5)
+    with pytest.raises(_lib.XmcError) as e:
+        t.run(n)
+    assert e.value.status == S.XMC_ERR_BUDGET
+    led = t.run(n, allow_budget=True)
+    assert led["n_budget"] > 0 and led["photons_terminated"] == n
+    assert ledger_identity_fx(led) == n * 2 ** 31
+    t.close()
+
+
+def test_cancel_stops_a_run(tmp_path):
+    xml, surf = scenes.planar(photons=1).write(str(tmp_path), "cancel")
+    m = api.Model(xml, surf)
+    t = api.Transport(m, roulette=True, area_kill=False)
+    n = 2_000_000_000
+    result = {}
+
+    def worker():
+        try:
+            result["led"] = t.run(n)
+        except _lib.XmcError as e:
+            result["err"] = e
+
+    th = threading.Thread(target=worker)
+    th.start()
+    time.sleep(1.0)
+    t.cancel()
+    th.join(timeout=60)
+    assert not th.is_alive()
+    assert "err" in result and result["err"].status == S.XMC_ERR_CANCELLED
+    t.close()
+
+
+def test_zero_photons_and_no_detectors(tmp_path):
+    sc = scenes.planar(photons=1, n_rings=0)
+    xml, surf = sc.write(str(tmp_path), "zero")
+    m = api.Model(xml, surf)
+    t = api.Transport(m)
+    led = t.run(0)
+    assert led["photons_launched"] == 0 and ledger_identity_fx(led) == 0
+    led = t.run(1000)
+    assert led["photons_terminated"] == 1000 and led["n_detected"] == 0
+    t.close()

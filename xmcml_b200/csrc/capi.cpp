@@ -1,0 +1,586 @@
+// C-ABI of the library: context creation (device image upload), runs, tally read-back and the
+// reference-signature shims. See include/xmcml_b200.h for the contract of each entry point.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "xmc_internal.h"
+
+namespace xmc {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+static int fail(int status, const std::string& msg) {
+    set_error(msg);
+    return status;
+}
+
+#define XMC_CUDA(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(XMC_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+static void free_context(Context* c) {
+    if (!c) return;
+    int dev = -1;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev != c->device) cudaSetDevice(c->device);
+    void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
+                     c->d_tbin, c->d_ledger, c->d_counter, c->d_status};
+    for (void* p : dbufs)
+        if (p) cudaFree(p);
+    void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status};
+    for (void* p : hbufs)
+        if (p) cudaFreeHost(p);
+    for (cudaEvent_t& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+// mcml_kernel.cpp:16-37 (FP64, exactly as the reference computes it)
+static double specular(const LayerInfo* layer) {
+    double r1, r2, t = (layer[0].refractiveIndex - layer[1].refractiveIndex) /
+                       (layer[0].refractiveIndex + layer[1].refractiveIndex);
+    r1 = t * t;
+    if (layer[1].absorptionCoefficient == 0.0 && layer[1].scatteringCoefficient == 0.0) {
+        t = (layer[1].refractiveIndex - layer[2].refractiveIndex) / (layer[1].refractiveIndex + layer[2].refractiveIndex);
+        r2 = t * t;
+        t = 1 - r1;
+        r1 = r1 + t * t * r2 / (1 - r1 * r2);
+    }
+    return r1;
+}
+
+static size_t smem_layout(int n_dets, int smem_nodes, int smem_tris, int smem_next) {
+    size_t b = sizeof(unsigned long long) * (size_t)(kLedgerSlots + 4 * n_dets);
+    b += sizeof(float4) * (size_t)(2 * smem_nodes + 3 * smem_tris);
+    b += sizeof(DevLayer) * MAX_LAYERS;
+    b += sizeof(DevDetector) * (size_t)n_dets;
+    b += (size_t)smem_next;
+    return (b + 15) & ~(size_t)15;
+}
+
+static int validate(const InputInfo* in, const xmc_options& opt) {
+    if (!in) return fail(XMC_ERR_INVALID_INPUT, "input is NULL");
+    if (in->numberOfLayers < 2 || in->numberOfLayers > MAX_LAYERS)
+        return fail(XMC_ERR_RANGE, "numberOfLayers must be in [2, " + std::to_string(MAX_LAYERS) + "]");
+    if (!in->layerInfo) return fail(XMC_ERR_INVALID_INPUT, "layerInfo is NULL");
+    if (!in->area) return fail(XMC_ERR_INVALID_INPUT, "area is NULL");
+    const Area& a = *in->area;
+    if (a.partitionNumber.x <= 0 || a.partitionNumber.y <= 0 || a.partitionNumber.z <= 0)
+        return fail(XMC_ERR_INVALID_INPUT, "Area partition numbers must be positive");
+    if (!(a.length.x > 0 && a.length.y > 0 && a.length.z > 0))
+        return fail(XMC_ERR_INVALID_INPUT, "Area lengths must be positive");
+    const int maxp = (opt.flags & XMC_LARGE_GRID) ? 4096 : 256;
+    if (a.partitionNumber.x > maxp || a.partitionNumber.y > maxp || a.partitionNumber.z > maxp)
+        return fail(XMC_ERR_RANGE, "Area partition number above " + std::to_string(maxp) +
+                                       " (the reference indexes voxels with bytes; set XMC_LARGE_GRID for full indices)");
+    if ((long long)a.partitionNumber.x * a.partitionNumber.y * a.partitionNumber.z > (1ll << 31) - 1)
+        return fail(XMC_ERR_RANGE, "Area grid too large");
+    if (in->numberOfSurfaces < 0 || (in->numberOfSurfaces > 0 && !in->surface))
+        return fail(XMC_ERR_INVALID_INPUT, "surfaces missing");
+    if (in->numberOfSurfaces > 4096) return fail(XMC_ERR_RANGE, "more than 4096 surfaces");
+    if (in->numberOfCubeDetectors < 0 || in->numberOfRingDetectors < 0 ||
+        (in->numberOfCubeDetectors > 0 && !in->cubeDetector) || (in->numberOfRingDetectors > 0 && !in->ringDetector))
+        return fail(XMC_ERR_INVALID_INPUT, "detectors missing");
+    if (in->numberOfCubeDetectors + in->numberOfRingDetectors > 1024) return fail(XMC_ERR_RANGE, "more than 1024 detectors");
+    if (in->timeScaleSize < 1) return fail(XMC_ERR_INVALID_INPUT, "timeScaleSize must be >= 1");
+    if ((long long)in->timeScaleSize * (in->numberOfCubeDetectors + in->numberOfRingDetectors) > (1ll << 26))
+        return fail(XMC_ERR_RANGE, "time-bin tally too large");
+    if (in->useBiasing) return fail(XMC_ERR_UNSUPPORTED, "biasing (attractive point) is not provided by the GPU path");
+    if (opt.flags & (XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ))
+        return fail(XMC_ERR_UNSUPPORTED, "scattering map and detector trajectory tallies are not provided by the GPU path");
+    for (int l = 0; l < in->numberOfLayers; ++l) {
+        const LayerInfo& L = in->layerInfo[l];
+        if (L.numberOfSurfaces < 0 || (L.numberOfSurfaces > 0 && !L.surfaceId))
+            return fail(XMC_ERR_INVALID_INPUT, "layer " + std::to_string(l) + ": surface ids missing");
+        if (!(L.refractiveIndex > 0)) return fail(XMC_ERR_INVALID_INPUT, "layer " + std::to_string(l) + ": refractive index must be > 0");
+        if (L.absorptionCoefficient < 0 || L.scatteringCoefficient < 0)
+            return fail(XMC_ERR_INVALID_INPUT, "layer " + std::to_string(l) + ": negative coefficients");
+    }
+    if (!(opt.roulette_chance > 0 && opt.roulette_chance <= 1)) return fail(XMC_ERR_INVALID_INPUT, "roulette_chance must be in (0, 1]");
+    if (opt.beam_radius < 0) return fail(XMC_ERR_INVALID_INPUT, "beam_radius must be >= 0");
+    return XMC_OK;
+}
+
+static int create(const InputInfo* in, const xmc_options* opt_in, Context** out) {
+    *out = nullptr;
+    xmc_options opt;
+    xmc_default_options(&opt);
+    if (opt_in && opt_in->struct_size) {
+        size_t n = std::min((size_t)opt_in->struct_size, sizeof(xmc_options));
+        std::memcpy(&opt, opt_in, n);
+        opt.struct_size = sizeof(xmc_options);
+        if (opt.roulette_chance == 0) opt.roulette_chance = 0.1;
+        if (opt.max_steps_per_photon == 0) opt.max_steps_per_photon = 10000000ull;
+        if (opt.photons_per_chunk <= 0) opt.photons_per_chunk = 256;
+    }
+    int st = validate(in, opt);
+    if (st) return st;
+
+    GeomImage geom;
+    std::string err;
+    if (!build_geometry(in, &geom, &err)) return fail(XMC_ERR_INVALID_INPUT, err);
+
+    Context* c = new (std::nothrow) Context();
+    if (!c) return fail(XMC_ERR_DEVICE, "out of host memory");
+    c->opt = opt;
+    c->device = opt.device;
+    auto bail = [&](int s) { free_context(c); return s; };
+    {
+        cudaError_t e = cudaSetDevice(c->device);
+        if (e != cudaSuccess) return bail(fail(XMC_ERR_DEVICE, std::string("cudaSetDevice: ") + cudaGetErrorString(e)));
+    }
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return bail(fail(XMC_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_))); \
+    } while (0)
+
+    KParams& kp = c->kp;
+    std::memset(&kp, 0, sizeof(kp));
+    // ---- layers ----
+    kp.n_layers = in->numberOfLayers;
+    for (int l = 0; l < MAX_LAYERS; ++l) {
+        DevLayer& D = kp.layer[l];
+        std::memset(&D, 0, sizeof(D));
+        if (l >= in->numberOfLayers) { D.glass = 1; D.n = 1.0f; continue; }
+        const LayerInfo& L = in->layerInfo[l];
+        const double mut = L.absorptionCoefficient + L.scatteringCoefficient;
+        const double g = L.anisotropy;
+        D.n = (float)L.refractiveIndex;
+        D.mua = (float)L.absorptionCoefficient;
+        D.mus = (float)L.scatteringCoefficient;
+        D.g = (float)g;
+        D.glass = (L.absorptionCoefficient == 0.0 && L.scatteringCoefficient == 0.0) ? 1 : 0;
+        D.inv_mut = D.glass ? 0.0f : (float)(1.0 / mut);
+        D.absorb = D.glass ? 0.0f : (float)(L.absorptionCoefficient / mut);
+        D.hg_a = (float)(1 - g * g);
+        D.hg_b = (float)(1 + g * g);
+        D.hg_c = g != 0.0 ? (float)(1.0 / (2 * g)) : 0.0f;
+        D.hg_d = (float)(1 - g);
+        D.hg_e = (float)(2 * g);
+    }
+    kp.target_mask = 0;
+    for (int l = 0; l < MAX_LAYERS; ++l)
+        if (in->targetRangeLayers[l]) kp.target_mask |= 1u << l;
+    // ---- surface -> layer transitions: FindIntersectionLayer (mcml_kernel.cpp:566-580) ----
+    const int ns = in->numberOfSurfaces;
+    std::vector<int8_t> next((size_t)std::max(1, ns) * MAX_LAYERS, (int8_t)-1);
+    for (int s = 0; s < ns; ++s)
+        for (int cur = 0; cur < MAX_LAYERS; ++cur) {
+            int found = -1;
+            for (int i = 0; i < in->numberOfLayers && found < 0; ++i)
+                for (int j = 0; j < in->layerInfo[i].numberOfSurfaces; ++j)
+                    if (in->layerInfo[i].surfaceId[j] == s && i != cur) { found = i; break; }
+            next[(size_t)s * MAX_LAYERS + cur] = (int8_t)found;
+        }
+    kp.n_surf = ns;
+    // ---- Area ----
+    const Area& A = *in->area;
+    kp.ax = (float)A.corner.x; kp.ay = (float)A.corner.y; kp.az = (float)A.corner.z;
+    kp.asx = (float)(A.partitionNumber.x / A.length.x);
+    kp.asy = (float)(A.partitionNumber.y / A.length.y);
+    kp.asz = (float)(A.partitionNumber.z / A.length.z);
+    kp.nx = A.partitionNumber.x; kp.ny = A.partitionNumber.y; kp.nz = A.partitionNumber.z;
+    kp.byte_sentinel = (A.partitionNumber.x >= 256 && A.partitionNumber.y >= 256 && A.partitionNumber.z >= 256 &&
+                        !(opt.flags & XMC_LARGE_GRID)) ? 1 : 0;
+    c->grid_size = A.partitionNumber.x * A.partitionNumber.y * A.partitionNumber.z;
+    // ---- detectors: cubes then rings (GetDetectorId order, mcml_kernel.cpp:663-742) ----
+    const int nd = in->numberOfCubeDetectors + in->numberOfRingDetectors;
+    std::vector<DevDetector> dets((size_t)std::max(1, nd));
+    const double kPi = 3.14159265358979323846;
+    for (int i = 0; i < in->numberOfCubeDetectors; ++i) {
+        const CubeDetector& D = in->cubeDetector[i];
+        DevDetector& o = dets[i];
+        o.cx = (float)D.center.x; o.cy = (float)D.center.y; o.cz = (float)D.center.z;
+        o.hx = (float)(D.length.x / 2.0); o.hy = (float)(D.length.y / 2.0); o.hz = (float)(D.length.z / 2.0);
+        o.cos_angle = (float)std::cos(D.targetAngle * kPi / 180.0);
+        o.filter = 0;
+        for (int j = 0; j < MAX_LAYERS; ++j) if (D.filterLayers[j]) o.filter |= 1u << j;
+    }
+    for (int i = 0; i < in->numberOfRingDetectors; ++i) {
+        const RingDetector& D = in->ringDetector[i];
+        DevDetector& o = dets[in->numberOfCubeDetectors + i];
+        o.cx = (float)D.center.x; o.cy = (float)D.center.y; o.cz = (float)D.center.z;
+        o.hx = (float)D.smallRadius; o.hy = (float)D.bigRadius; o.hz = 0.0f;
+        o.cos_angle = (float)std::cos(D.targetAngle * kPi / 180.0);
+        o.filter = 0;
+        for (int j = 0; j < MAX_LAYERS; ++j) if (D.filterLayers[j]) o.filter |= 1u << j;
+    }
+    kp.n_cubes = in->numberOfCubeDetectors;
+    kp.n_rings = in->numberOfRingDetectors;
+    kp.n_dets = nd;
+    c->n_dets = nd;
+    // ---- time bins: InitOutput (launcher_omp.cpp:36-55) ----
+    const int T = in->timeScaleSize;
+    double tstep = (in->timeFinish - in->timeStart) / T;
+    if (tstep < 0.0) tstep = 0.0;
+    c->bin_start.resize(T);
+    c->bin_finish.resize(T);
+    for (int j = 0; j < T - 1; ++j) {
+        c->bin_start[j] = in->timeStart + j * tstep;
+        c->bin_finish[j] = c->bin_start[j] + tstep;
+    }
+    c->bin_start[T - 1] = in->timeStart + (T - 1) * tstep;
+    c->bin_finish[T - 1] = in->timeFinish;
+    kp.t0 = (float)in->timeStart;
+    kp.dt = (float)tstep;
+    kp.n_time = T;
+    c->n_time = T;
+    // ---- launch (mcml_kernel.cpp:128-149) ----
+    c->rsp = specular(in->layerInfo);
+    const double w0 = 1.0 - c->rsp;
+    c->w0_fx = (uint32_t)std::llround(w0 * kWeightScale);
+    kp.w0 = c->w0_fx;
+    {
+        double wm = std::ceil(in->minWeight * kWeightScale);
+        if (!(wm > 0)) wm = 0;
+        if (wm > 4294967295.0) wm = 4294967295.0;
+        kp.w_min = (uint32_t)wm;
+    }
+    kp.sx = (float)in->startPosition.x;
+    kp.sy = (float)in->startPosition.y;
+    kp.sz = (float)(in->startPosition.z + 1.0e-8);
+    kp.dx = (float)in->startDirection.x;
+    kp.dy = (float)in->startDirection.y;
+    kp.dz = (float)in->startDirection.z;
+    kp.beam_radius = (float)opt.beam_radius;
+    kp.chance = (float)opt.roulette_chance;
+    kp.inv_chance = (float)(1.0 / opt.roulette_chance);
+    kp.flags = opt.flags;
+    kp.max_steps = opt.max_steps_per_photon;
+    kp.chunk = opt.photons_per_chunk;
+
+    // ---- shared-memory staging plan ----
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, c->device));
+    c->num_sms = prop.multiProcessorCount;
+    const size_t smem_cap = 48 * 1024;  // per block, leaves room for several blocks per SM
+    int smem_next = (int)std::min<size_t>((size_t)ns * MAX_LAYERS, 4096);
+    int smem_tris = geom.n_tris <= 256 ? geom.n_tris : 0;
+    int smem_nodes = 0;
+    if (opt.smem_nodes >= 0) {
+        size_t base = smem_layout(nd, 0, smem_tris, smem_next);
+        if (base < smem_cap) smem_nodes = (int)std::min<size_t>((smem_cap - base) / 32, (size_t)geom.n_nodes);
+        if (opt.smem_nodes > 0) smem_nodes = std::min(smem_nodes, opt.smem_nodes);
+    }
+    kp.smem_nodes = smem_nodes;
+    kp.smem_tris = smem_tris;
+    kp.smem_next = smem_next;
+    kp.n_nodes = geom.n_nodes;
+    kp.n_tris = geom.n_tris;
+    c->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next);
+
+    // ---- device buffers ----
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : c->ev) CK(cudaEventCreate(&e));
+    auto up = [&](void** d, const void* h, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(d, bytes ? bytes : 16);
+        if (e != cudaSuccess) return e;
+        if (bytes) e = cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, c->stream);
+        return e;
+    };
+    c->h2d_bytes = sizeof(float4) * (geom.nodes.size() + geom.tris.size()) + next.size() + sizeof(DevDetector) * dets.size();
+    CK(up(&c->d_nodes, geom.nodes.data(), sizeof(float4) * geom.nodes.size()));
+    CK(up(&c->d_tris, geom.tris.data(), sizeof(float4) * geom.tris.size()));
+    CK(up(&c->d_next, next.data(), next.size()));
+    CK(up(&c->d_dets, dets.data(), sizeof(DevDetector) * dets.size()));
+    const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
+    const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, nd);
+    const size_t tbin_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, nd) * T;
+    const size_t led_b = sizeof(unsigned long long) * kLedgerSlots;
+    CK(cudaMalloc(&c->d_absorb, absorb_b));
+    CK(cudaMalloc(&c->d_det, det_b));
+    CK(cudaMalloc(&c->d_tbin, tbin_b));
+    CK(cudaMalloc(&c->d_ledger, led_b));
+    CK(cudaMalloc(&c->d_counter, 16));
+    CK(cudaMalloc(&c->d_status, 16));
+    CK(cudaHostAlloc((void**)&c->h_cancel, 16, cudaHostAllocMapped));
+    *c->h_cancel = 0;
+    CK(cudaHostAlloc((void**)&c->h_absorb, absorb_b, cudaHostAllocDefault));
+    CK(cudaHostAlloc((void**)&c->h_det, det_b, cudaHostAllocDefault));
+    CK(cudaHostAlloc((void**)&c->h_tbin, tbin_b, cudaHostAllocDefault));
+    CK(cudaHostAlloc((void**)&c->h_ledger, led_b, cudaHostAllocDefault));
+    CK(cudaHostAlloc((void**)&c->h_status, 16, cudaHostAllocDefault));
+    int* d_cancel = nullptr;
+    CK(cudaHostGetDevicePointer((void**)&d_cancel, c->h_cancel, 0));
+    kp.nodes = (const float4*)c->d_nodes;
+    kp.tris = (const float4*)c->d_tris;
+    kp.next_layer = (const int8_t*)c->d_next;
+    kp.dets = (const DevDetector*)c->d_dets;
+    kp.absorb = (unsigned long long*)c->d_absorb;
+    kp.det = (unsigned long long*)c->d_det;
+    kp.tbin = (unsigned long long*)c->d_tbin;
+    kp.ledger = (unsigned long long*)c->d_ledger;
+    kp.counter = (unsigned long long*)c->d_counter;
+    kp.cancel = d_cancel;
+    kp.status = (int*)c->d_status;
+
+    // ---- launch shape ----
+    c->block = opt.block_size > 0 ? opt.block_size : 256;
+    if (c->block % 32 != 0 || c->block > 1024) return bail(fail(XMC_ERR_INVALID_INPUT, "block_size must be a multiple of 32 <= 1024"));
+    int occ = 0;
+    CK(transport_occupancy(c->block, c->smem_bytes, &occ));
+    if (occ <= 0) return bail(fail(XMC_ERR_DEVICE, "transport kernel cannot be resident with this block size / shared memory"));
+    c->blocks_per_sm = opt.blocks_per_sm > 0 ? std::min(opt.blocks_per_sm, occ) : occ;
+    c->grid = c->num_sms * c->blocks_per_sm;
+    CK(cudaStreamSynchronize(c->stream));
+#undef CK
+    *out = c;
+    return XMC_OK;
+}
+
+static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo* out, xmc_ledger* led) {
+    XMC_CUDA(cudaSetDevice(c->device));
+    KParams& kp = c->kp;
+    kp.key0 = (uint32_t)seed;
+    kp.key1 = (uint32_t)(seed >> 32);
+    kp.first_id = first;
+    kp.n_photons = n;
+    *c->h_cancel = 0;
+    const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
+    const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, c->n_dets);
+    const size_t tbin_b = det_b * c->n_time;
+    const size_t led_b = sizeof(unsigned long long) * kLedgerSlots;
+    XMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    XMC_CUDA(cudaMemsetAsync(c->d_absorb, 0, absorb_b, c->stream));
+    XMC_CUDA(cudaMemsetAsync(c->d_det, 0, det_b, c->stream));
+    XMC_CUDA(cudaMemsetAsync(c->d_tbin, 0, tbin_b, c->stream));
+    XMC_CUDA(cudaMemsetAsync(c->d_ledger, 0, led_b, c->stream));
+    XMC_CUDA(cudaMemsetAsync(c->d_counter, 0, 16, c->stream));
+    XMC_CUDA(cudaMemsetAsync(c->d_status, 0, 16, c->stream));
+    XMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    if (n > 0) XMC_CUDA(enqueue_transport(c));
+    XMC_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    if (out) XMC_CUDA(cudaMemcpyAsync(c->h_absorb, c->d_absorb, absorb_b, cudaMemcpyDeviceToHost, c->stream));
+    XMC_CUDA(cudaMemcpyAsync(c->h_det, c->d_det, det_b, cudaMemcpyDeviceToHost, c->stream));
+    if (out) XMC_CUDA(cudaMemcpyAsync(c->h_tbin, c->d_tbin, tbin_b, cudaMemcpyDeviceToHost, c->stream));
+    XMC_CUDA(cudaMemcpyAsync(c->h_ledger, c->d_ledger, led_b, cudaMemcpyDeviceToHost, c->stream));
+    XMC_CUDA(cudaMemcpyAsync(c->h_status, c->d_status, 16, cudaMemcpyDeviceToHost, c->stream));
+    XMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    XMC_CUDA(cudaStreamSynchronize(c->stream));
+    float k_ms = 0, t_ms = 0;
+    XMC_CUDA(cudaEventElapsedTime(&k_ms, c->ev[1], c->ev[2]));
+    XMC_CUDA(cudaEventElapsedTime(&t_ms, c->ev[0], c->ev[3]));
+    c->last_kernel_ms = k_ms;
+    c->last_total_ms = t_ms;
+    c->last_n = n;
+
+    const unsigned long long* L = c->h_ledger;
+    const double inv_scale = 1.0 / kWeightScale;
+    if (out) {
+        if (out->gridSize != c->grid_size) return fail(XMC_ERR_INVALID_INPUT, "output gridSize does not match the input Area");
+        if (out->numberOfDetectors != c->n_dets) return fail(XMC_ERR_INVALID_INPUT, "output numberOfDetectors does not match the input");
+        out->specularReflectance = c->rsp;
+        if (out->absorption)
+            for (int i = 0; i < c->grid_size; ++i) out->absorption[i] += (double)c->h_absorb[i] * inv_scale;
+        for (int d = 0; d < c->n_dets; ++d) {
+            DetectorInfo& D = out->detectorInfo[d];
+            const unsigned long long* t = c->h_det + 4 * (size_t)d;
+            D.weight += (double)t[0] * inv_scale;
+            D.numberOfPhotons += t[1];
+            D.targetWeight += (double)t[2] * inv_scale;
+            if (D.timeScale && D.timeScaleSize == c->n_time) {
+                for (int j = 0; j < c->n_time; ++j) {
+                    const unsigned long long* b = c->h_tbin + 4 * ((size_t)d * c->n_time + j);
+                    D.timeScale[j].weight += (double)b[0] * inv_scale;
+                    D.timeScale[j].numberOfPhotons += b[1];
+                    D.timeScale[j].targetWeight += (double)b[2] * inv_scale;
+                }
+            }
+        }
+    }
+    if (led) {
+        std::memset(led, 0, sizeof(*led));
+        led->photons_launched = L[L_LAUNCHED];
+        led->photons_terminated = L[L_TERMINATED];
+        led->steps = L[L_STEPS];
+        led->n_escaped_top = L[L_N_TOP];
+        led->n_escaped_bottom = L[L_N_BOTTOM];
+        led->n_area = L[L_N_AREA];
+        led->n_cut = L[L_N_CUT];
+        led->n_roulette = L[L_N_ROULETTE];
+        led->n_glass = L[L_N_GLASS];
+        led->n_budget = L[L_N_BUDGET];
+        led->n_invalid = L[L_N_INVALID];
+        led->n_detected = L[L_N_DETECTED];
+        led->n_fp64_retests = L[L_N_RETEST];
+        led->n_node_visits = L[L_N_NODES];
+        led->n_triangle_tests = L[L_N_TRIS];
+        led->specular_fx = (unsigned long long)(kWeightOne - c->w0_fx) * L[L_LAUNCHED];
+        led->absorbed_fx = L[L_ABSORBED];
+        led->absorbed_outside_fx = L[L_ABSORBED_OUT];
+        led->escaped_top_fx = L[L_TOP];
+        led->escaped_bottom_fx = L[L_BOTTOM];
+        led->lost_area_fx = L[L_AREA];
+        led->lost_cut_fx = L[L_CUT];
+        led->lost_glass_fx = L[L_GLASS];
+        led->lost_budget_fx = L[L_BUDGET];
+        led->lost_invalid_fx = L[L_INVALID];
+        led->roulette_killed_fx = L[L_RKILLED];
+        led->roulette_gained_fx = L[L_RGAINED];
+        const double np = n > 0 ? (double)n : 1.0;
+        const double s = inv_scale / np;
+        led->specular = (double)led->specular_fx * s;
+        led->absorbed = (double)led->absorbed_fx * s;
+        led->absorbed_outside = (double)led->absorbed_outside_fx * s;
+        led->escaped_top = (double)led->escaped_top_fx * s;
+        led->escaped_bottom = (double)led->escaped_bottom_fx * s;
+        led->lost_area = (double)led->lost_area_fx * s;
+        led->lost_cut = (double)led->lost_cut_fx * s;
+        led->lost_glass = (double)led->lost_glass_fx * s;
+        led->lost_budget = (double)led->lost_budget_fx * s;
+        led->lost_invalid = (double)led->lost_invalid_fx * s;
+        led->roulette_killed = (double)led->roulette_killed_fx * s;
+        led->roulette_gained = (double)led->roulette_gained_fx * s;
+        led->kernel_ms = k_ms;
+        led->total_ms = t_ms;
+        led->h2d_bytes = c->h2d_bytes + sizeof(KParams);
+        led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16;
+    }
+    if (c->h_status[0] & 2) return fail(XMC_ERR_CANCELLED, "run cancelled");
+    if (c->h_status[0] & 1) return fail(XMC_ERR_BUDGET, "a photon reached the step budget and was terminated");
+    return XMC_OK;
+}
+
+}  // namespace xmc
+
+using namespace xmc;
+
+extern "C" {
+
+int xmc_version(void) { return 10000 * 0 + 100 * 1 + 0; }
+
+const char* xmc_last_error(void) { return g_last_error.c_str(); }
+
+void xmc_default_options(xmc_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(xmc_options);
+    o->roulette_chance = 0.1;
+    o->max_steps_per_photon = 10000000ull;
+    o->photons_per_chunk = 256;
+}
+
+int xmc_create(const InputInfo* input, const xmc_options* opt, xmc_context** out_ctx) {
+    if (!out_ctx) return fail(XMC_ERR_INVALID_INPUT, "out_ctx is NULL");
+    set_error("");
+    Context* c = nullptr;
+    int st = create(input, opt, &c);
+    *out_ctx = reinterpret_cast<xmc_context*>(c);
+    return st;
+}
+
+int xmc_run(xmc_context* ctx, uint64_t seed, uint64_t first_photon_id, uint64_t n_photons, OutputInfo* output,
+            xmc_ledger* ledger) {
+    if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
+    return run(reinterpret_cast<Context*>(ctx), seed, first_photon_id, n_photons, output, ledger);
+}
+
+int xmc_read_tallies(xmc_context* ctx, uint64_t* absorption, uint64_t* det_weight, uint64_t* det_count,
+                     uint64_t* det_target, uint64_t* det_weight2, uint64_t* time_weight, uint64_t* time_count,
+                     uint64_t* time_target, uint64_t* time_weight2) {
+    if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
+    Context* c = reinterpret_cast<Context*>(ctx);
+    XMC_CUDA(cudaSetDevice(c->device));
+    const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
+    const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, c->n_dets);
+    const size_t tbin_b = det_b * c->n_time;
+    XMC_CUDA(cudaMemcpyAsync(c->h_absorb, c->d_absorb, absorb_b, cudaMemcpyDeviceToHost, c->stream));
+    XMC_CUDA(cudaMemcpyAsync(c->h_det, c->d_det, det_b, cudaMemcpyDeviceToHost, c->stream));
+    XMC_CUDA(cudaMemcpyAsync(c->h_tbin, c->d_tbin, tbin_b, cudaMemcpyDeviceToHost, c->stream));
+    XMC_CUDA(cudaStreamSynchronize(c->stream));
+    if (absorption) std::memcpy(absorption, c->h_absorb, absorb_b);
+    for (int d = 0; d < c->n_dets; ++d) {
+        const unsigned long long* t = c->h_det + 4 * (size_t)d;
+        if (det_weight) det_weight[d] = t[0];
+        if (det_count) det_count[d] = t[1];
+        if (det_target) det_target[d] = t[2];
+        if (det_weight2) det_weight2[d] = t[3];
+        for (int j = 0; j < c->n_time; ++j) {
+            const unsigned long long* b = c->h_tbin + 4 * ((size_t)d * c->n_time + j);
+            const size_t k = (size_t)d * c->n_time + j;
+            if (time_weight) time_weight[k] = b[0];
+            if (time_count) time_count[k] = b[1];
+            if (time_target) time_target[k] = b[2];
+            if (time_weight2) time_weight2[k] = b[3];
+        }
+    }
+    return XMC_OK;
+}
+
+int xmc_cancel(xmc_context* ctx) {
+    if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
+    Context* c = reinterpret_cast<Context*>(ctx);
+    *(volatile int*)c->h_cancel = 1;
+    return XMC_OK;
+}
+
+int xmc_destroy(xmc_context* ctx) {
+    free_context(reinterpret_cast<Context*>(ctx));
+    return XMC_OK;
+}
+
+int xmc_launch(const InputInfo* input, OutputInfo* output, uint64_t seed, uint64_t first_photon_id,
+               const xmc_options* opt, xmc_ledger* ledger) {
+    xmc_context* c = nullptr;
+    int st = xmc_create(input, opt, &c);
+    if (st) return st;
+    st = xmc_run(c, seed, first_photon_id, input->numberOfPhotons, output, ledger);
+    std::string keep = g_last_error;
+    xmc_destroy(c);
+    set_error(keep);
+    return st;
+}
+
+int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* rng, int numThreads) {
+    (void)numThreads;
+    if (!input || !output || !rng) {
+        set_error("xmc_launch_omp: NULL argument");
+        std::fprintf(stderr, "xmc_launch_omp: %s\n", xmc_last_error());
+        return XMC_ERR_INVALID_INPUT;
+    }
+    int st = xmc_launch(input, output, rng[0].value, 0, nullptr, nullptr);
+    if (st && st != XMC_ERR_BUDGET) {
+        std::fprintf(stderr, "xmc_launch_omp: %s\n", xmc_last_error());
+        return st;
+    }
+    // advance the caller's generator by one MCG59 step (mcml_mcg59.cpp:34-38) so the next call
+    // (the next backup portion) uses a fresh key
+    rng[0].value = (rng[0].value * rng[0].offset) & 576460752303423487ULL;
+    return st;
+}
+
+double xmc_specular_reflectance(const LayerInfo* layer) { return specular(layer); }
+
+void xmc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c1 = (uint32_t)p1;
+        c3 = (uint32_t)p0;
+        c0 = n0;
+        c2 = n2;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+int xmc_device_philox(uint64_t seed, uint64_t photon_id, uint32_t n, uint32_t* out) {
+    XMC_CUDA(device_philox((uint32_t)seed, (uint32_t)(seed >> 32), photon_id, n, out));
+    return XMC_OK;
+}
+
+}  // extern "C"

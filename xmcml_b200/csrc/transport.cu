@@ -1,0 +1,491 @@
+// Persistent photon-transport kernel for sm_100a: the GPU counterpart of the reference's
+// ComputePhoton walk (base/xmcml/xmcml/mcml_kernel.cpp:39-126) driven by LaunchOMP's photon loop
+// (base/xmcml/xmcmlLauncher/launcher_omp.cpp:138-144).
+//
+// One thread walks one photon at a time; a warp claims photon ids in chunks from a global
+// dispenser and refills lanes whose photon died before the next iteration (warp-level compaction
+// of live photons), so lanes stay busy until the dispenser runs dry. Every random number comes
+// from Philox4x32-10 keyed by the seed with counter (photon id, iteration, 0): one block of four
+// 24-bit uniforms per walk iteration, with fixed slots, so a photon's path does not depend on
+// which thread runs it and the tallies (64-bit fixed-point integer sums) are bit-identical for
+// every launch shape.
+//
+// Per iteration (tissue layer): slot 0 step length; on a boundary hit slot 1 Fresnel test and
+// slot 2 roulette; on an interaction slot 1 HG cos(theta), slot 2 azimuth, slot 3 roulette.
+// Glass layer: slot 0 Fresnel test, slot 1 roulette. The photon-weight arithmetic is integer
+// (weight 1.0 == 2^31): every deposit is subtracted from the photon's integer weight, so the
+// ledger terms add up to launched weight exactly.
+#include <cstdint>
+
+#include "geom.cuh"
+#include "xmc_internal.h"
+
+namespace xmc {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// 24-bit uniform in (0,1), exactly the value the FP64 oracle uses.
+__device__ __forceinline__ float u24(uint32_t x) { return fmaf((float)(x >> 8), 0x1p-24f, 0x1p-25f); }
+
+struct Photon {
+    float px, py, pz, dx, dy, dz;
+    float time, trange, orange;
+    uint32_t w;
+    int layer;
+    uint32_t visited;
+    uint32_t iter;
+    int excl;
+    float tmin;
+    unsigned long long pid;
+};
+
+// GetAreaIndex (mcml_kernel.cpp:190-227): voxel of a point, -1 outside Area. `tol` (voxel units)
+// widens the box for points on a surface: the reference stops 1e-10 mm in front of a surface
+// (mcml_kernel.cpp:60,87), so a surface lying on an Area face counts as inside; the FP32 hit point
+// sits on the surface within rounding and is accepted within tol, clamped to the edge voxel.
+__device__ __forceinline__ int area_index(const KParams& P, float x, float y, float z, float tol) {
+    float fx = (x - P.ax) * P.asx, fy = (y - P.ay) * P.asy, fz = (z - P.az) * P.asz;
+    if (!(fx >= -tol && fy >= -tol && fz >= -tol)) return -1;
+    if (!(fx < (float)P.nx + tol && fy < (float)P.ny + tol && fz < (float)P.nz + tol)) return -1;
+    const int ix = min(max((int)fx, 0), P.nx - 1), iy = min(max((int)fy, 0), P.ny - 1), iz = min(max((int)fz, 0), P.nz - 1);
+    if (P.byte_sentinel && ix == 255 && iy == 255 && iz == 255) return -1;
+    return (ix * P.ny + iy) * P.nz + iz;
+}
+
+// Block-private tallies in shared memory.
+struct SmemTally {
+    unsigned long long* ledger;  // [kLedgerSlots]
+    unsigned long long* det;     // [n_dets * 4]
+};
+
+__device__ __forceinline__ void lat(unsigned long long* p, unsigned long long v) {
+    if (v) atomicAdd(p, v);
+}
+
+// mcml_kernel.cpp:663-742 (first matching cube, then ring; layer filter; angle test) and the
+// detector tallies of :744-858. Weight arithmetic in fixed point.
+__device__ void detect_and_tally(const KParams& P, const SmemTally& S, const DevDetector* __restrict__ s_det,
+                                 const Photon& ph) {
+    int det = -1;
+    const float l2 = ph.dx * ph.dx + ph.dy * ph.dy + ph.dz * ph.dz;
+    const float ac = -ph.dz / l2;
+    for (int i = 0; i < P.n_dets; ++i) {
+        const DevDetector D = s_det[i];
+        bool inside;
+        if (i < P.n_cubes) {
+            inside = ph.px >= D.cx - D.hx && ph.px < D.cx + D.hx && ph.py >= D.cy - D.hy && ph.py < D.cy + D.hy &&
+                     ph.pz >= D.cz - D.hz && ph.pz < D.cz + D.hz;
+        } else {
+            const float ex = ph.px - D.cx, ey = ph.py - D.cy;
+            const float r = sqrtf(ex * ex + ey * ey);
+            inside = r >= D.hx && r < D.hy;
+        }
+        if (inside && (D.filter & ph.visited) && ac > D.cos_angle) {
+            det = i;
+            break;
+        }
+    }
+    if (det < 0) return;
+    const uint32_t w = ph.w;
+    const float total = ph.trange + ph.orange;
+    const uint32_t tw = total > 0.0f ? __float2uint_rn(__uint2float_rn(w) * (ph.trange / total)) : 0u;
+    const unsigned long long w2 = ((unsigned long long)w * w) >> 31;
+    atomicAdd(&S.det[4 * det + 0], (unsigned long long)w);
+    atomicAdd(&S.det[4 * det + 1], 1ull);
+    lat(&S.det[4 * det + 2], tw);
+    lat(&S.det[4 * det + 3], w2);
+    atomicAdd(&S.ledger[L_N_DETECTED], 1ull);
+    // time bins (mcml_kernel.cpp:812-849): [t0 + i dt, t0 + (i+1) dt), last bin open-ended
+    if (ph.time >= P.t0) {
+        int bin = P.n_time - 1;
+        if (P.dt > 0.0f) {
+            const float f = (ph.time - P.t0) / P.dt;
+            if (f < (float)(P.n_time - 1)) bin = (int)f;
+        }
+        unsigned long long* tb = P.tbin + 4 * ((size_t)det * P.n_time + bin);
+        atomicAdd(tb + 0, (unsigned long long)w);
+        atomicAdd(tb + 1, 1ull);
+        lat(tb + 2, tw);
+        lat(tb + 3, w2);
+    }
+}
+
+__device__ __forceinline__ void kill(const SmemTally& S, Photon& ph, bool& alive, int count_slot, int weight_slot) {
+    atomicAdd(&S.ledger[count_slot], 1ull);
+    lat(&S.ledger[weight_slot], ph.w);
+    atomicAdd(&S.ledger[L_TERMINATED], 1ull);
+    alive = false;
+}
+
+__device__ __forceinline__ void launch_photon(const KParams& P, Photon& ph, unsigned long long pid) {
+    ph.pid = pid;
+    ph.px = P.sx;
+    ph.py = P.sy;
+    ph.pz = P.sz;
+    if (P.beam_radius > 0.0f) {
+        const uint4 r = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), 0u, 1u), P.key0, P.key1);
+        const float rad = P.beam_radius * sqrtf(u24(r.x));
+        float a = u24(r.y);
+        a = a > 0.5f ? a - 1.0f : a;
+        float sp, cp;
+        __sincosf(6.283185307179586f * a, &sp, &cp);
+        ph.px += rad * cp;
+        ph.py += rad * sp;
+    }
+    ph.dx = P.dx;
+    ph.dy = P.dy;
+    ph.dz = P.dz;
+    ph.time = 0.0f;
+    ph.trange = 0.0f;
+    ph.orange = 0.0f;
+    ph.w = P.w0;
+    ph.layer = 1;
+    ph.visited = 1u << 1;
+    ph.iter = 0;
+    ph.excl = -1;
+    ph.tmin = kTminAfter;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    // --- shared memory carve-up (must match smem_layout on the host) ---
+    unsigned long long* s_ledger = reinterpret_cast<unsigned long long*>(smem);
+    unsigned long long* s_dettal = s_ledger + kLedgerSlots;
+    float4* s_nodes = reinterpret_cast<float4*>(s_dettal + 4 * P.n_dets);
+    float4* s_tris = s_nodes + 2 * P.smem_nodes;
+    DevLayer* s_layer = reinterpret_cast<DevLayer*>(s_tris + 3 * P.smem_tris);
+    DevDetector* s_det = reinterpret_cast<DevDetector*>(s_layer + MAX_LAYERS);
+    int8_t* s_next = reinterpret_cast<int8_t*>(s_det + P.n_dets);
+
+    for (int i = threadIdx.x; i < kLedgerSlots + 4 * P.n_dets; i += blockDim.x) s_ledger[i] = 0ull;
+    for (int i = threadIdx.x; i < 2 * P.smem_nodes; i += blockDim.x) s_nodes[i] = __ldg(&P.nodes[i]);
+    for (int i = threadIdx.x; i < 3 * P.smem_tris; i += blockDim.x) s_tris[i] = __ldg(&P.tris[i]);
+    for (int i = threadIdx.x; i < MAX_LAYERS; i += blockDim.x) s_layer[i] = P.layer[i];
+    for (int i = threadIdx.x; i < P.n_dets; i += blockDim.x) s_det[i] = P.dets[i];
+    for (int i = threadIdx.x; i < P.smem_next; i += blockDim.x) s_next[i] = P.next_layer[i];
+    __syncthreads();
+    const SmemTally S{s_ledger, s_dettal};
+
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const bool area_kill = !(P.flags & XMC_NO_AREA_KILL);
+    const bool roulette = (P.flags & XMC_ROULETTE) != 0;
+
+    unsigned long long cbeg = 0, cend = 0;  // warp-uniform chunk of photon indices
+    bool exhausted = false;                 // warp-uniform
+    bool alive = false;
+    Photon ph;
+    unsigned steps = 0, retests = 0, n_visit = 0, n_tri = 0;
+    unsigned budget_hit = 0;
+
+    for (;;) {
+        // ---- refill dead lanes with new photons (warp-level compaction) ----
+        unsigned need = __ballot_sync(FULL, !alive && !exhausted);
+        while (need) {
+            if (cbeg == cend) {
+                unsigned long long b = 0;
+                int cancelled = 0;
+                if (lane == 0) {
+                    if (P.cancel && *P.cancel) cancelled = 1;
+                    b = cancelled ? P.n_photons : atomicAdd(P.counter, (unsigned long long)P.chunk);
+                }
+                b = __shfl_sync(FULL, b, 0);
+                cancelled = __shfl_sync(FULL, cancelled, 0);
+                if (cancelled && lane == 0) atomicOr(P.status, 2);
+                if (b >= P.n_photons) {
+                    exhausted = true;
+                    break;
+                }
+                cbeg = b;
+                cend = min(b + (unsigned long long)P.chunk, P.n_photons);
+            }
+            const unsigned long long avail = cend - cbeg;
+            const int rank = __popc(need & lt_mask);
+            const int cnt = __popc(need);
+            const int take = (int)min((unsigned long long)cnt, avail);
+            if (((need >> lane) & 1u) && rank < take) {
+                launch_photon(P, ph, P.first_id + cbeg + rank);
+                alive = true;
+                atomicAdd(&S.ledger[L_LAUNCHED], 1ull);
+            }
+            cbeg += take;
+            need = __ballot_sync(FULL, !alive && !exhausted);
+        }
+        if (__ballot_sync(FULL, alive) == 0u) break;
+        if (!alive) continue;
+
+        // ---- one walk iteration (mcml_kernel.cpp:47-125) ----
+        if (ph.iter >= P.max_steps) {
+            budget_hit = 1;
+            kill(S, ph, alive, L_N_BUDGET, L_BUDGET);
+            continue;
+        }
+        const uint4 r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter, 0u), P.key0, P.key1);
+        ph.iter++;
+        steps++;
+        const DevLayer L = s_layer[ph.layer];
+        float u_roulette;
+        bool boundary;
+        Hit hit;
+        float step;
+        if (L.glass) {
+            hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py, ph.pz,
+                              ph.dx, ph.dy, ph.dz, ph.tmin, INFINITY, ph.excl, retests, n_visit, n_tri);
+            boundary = true;
+            u_roulette = u24(r.y);
+            if (hit.tri < 0) {
+                kill(S, ph, alive, L_N_GLASS, L_GLASS);
+                continue;
+            }
+            step = hit.t;
+        } else {
+            step = -__logf(u24(r.x)) * L.inv_mut;  // mcml_kernel.cpp:618-631
+            hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py, ph.pz,
+                              ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
+            boundary = hit.tri >= 0;
+            if (boundary) step = hit.t;
+            u_roulette = boundary ? u24(r.z) : u24(r.w);
+        }
+        // move (mcml_kernel.cpp:151-174): optical path length, target/other range
+        ph.px = fmaf(step, ph.dx, ph.px);
+        ph.py = fmaf(step, ph.dy, ph.py);
+        ph.pz = fmaf(step, ph.dz, ph.pz);
+        ph.time = fmaf(step, L.n, ph.time);
+        if ((P.target_mask >> ph.layer) & 1u) ph.trange += step;
+        else ph.orange += step;
+        const int idx = area_index(P, ph.px, ph.py, ph.pz, boundary ? 1e-4f : 0.0f);
+        if (idx < 0 && area_kill) {  // outside Area: the reference kills the photon (:63-76, :90-117)
+            kill(S, ph, alive, L_N_AREA, L_AREA);
+            continue;
+        }
+        if (boundary) {
+            // ---- CrossBoundary (mcml_kernel.cpp:229-284) ----
+            const float4 a = hit.tri < P.smem_tris ? s_tris[3 * hit.tri] : __ldg(&P.tris[3 * hit.tri]);
+            const float4 b = hit.tri < P.smem_tris ? s_tris[3 * hit.tri + 1] : __ldg(&P.tris[3 * hit.tri + 1]);
+            const float4 c = hit.tri < P.smem_tris ? s_tris[3 * hit.tri + 2] : __ldg(&P.tris[3 * hit.tri + 2]);
+            // GetPlaneNormal (mcml_math.cpp:45-50), normalised
+            const float e1x = a.x - b.x, e1y = a.y - b.y, e1z = a.z - b.z;
+            const float e2x = a.x - c.x, e2y = a.y - c.y, e2z = a.z - c.z;
+            float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+            const float nr = rsqrtf(nx * nx + ny * ny + nz * nz);
+            nx *= nr; ny *= nr; nz *= nr;
+            const int surf = __float_as_int(a.w);
+            const int next = surf * MAX_LAYERS + ph.layer < P.smem_next ? (int)s_next[surf * MAX_LAYERS + ph.layer]
+                                                                         : (int)__ldg(&P.next_layer[surf * MAX_LAYERS + ph.layer]);
+            if (next < 0) {
+                kill(S, ph, alive, L_N_INVALID, L_INVALID);
+                continue;
+            }
+            const float ni = L.n, nt = s_layer[next].n;
+            const float dn = ph.dx * nx + ph.dy * ny + ph.dz * nz;
+            const float ci = fabsf(dn);
+            float R;
+            if (ni == nt) {
+                R = 0.0f;
+            } else {
+                // GetCriticalCos (mcml_kernel.cpp:644-661)
+                const float cc = ni > nt ? sqrtf(1.0f - (nt * nt) / (ni * ni)) : 0.0f;
+                if (ci <= cc) {
+                    R = 1.0f;
+                } else if (ci > 1.0f - 1e-6f) {
+                    R = (nt - ni) / (nt + ni);
+                    R *= R;
+                } else if (ci < 1e-6f) {
+                    R = 1.0f;
+                } else if (ni > nt && ci - cc < 1e-3f) {
+                    // near the critical angle: ComputeTransmitCosine + ComputeFrenselReflectance in FP64
+                    const double Ci = ci, Ni = ni, Nt = nt;
+                    const double Si = sqrt(1.0 - Ci * Ci);
+                    const double St = Ni * Si / Nt;
+                    if (St >= 1.0) {
+                        R = 1.0f;
+                    } else {
+                        const double Ct = sqrt(1.0 - St * St);
+                        const double cs = Ci * Ct - Si * St, cd = Ci * Ct + Si * St;
+                        const double ss = Si * Ct + Ci * St, sd = Si * Ct - Ci * St;
+                        R = (float)(0.5 * sd * sd * (cd * cd + cs * cs) / (ss * ss * cd * cd));
+                    }
+                } else {
+                    // ComputeTransmitCosine / ComputeFrenselReflectance (mcml_kernel.cpp:497-564)
+                    const float si = sqrtf(1.0f - ci * ci);
+                    const float st = ni * si / nt;
+                    if (st >= 1.0f) {
+                        R = 1.0f;
+                    } else {
+                        const float ct = sqrtf(1.0f - st * st);
+                        const float cs = ci * ct - si * st, cd = ci * ct + si * st;
+                        const float ss = si * ct + ci * st, sd = si * ct - ci * st;
+                        R = 0.5f * sd * sd * (cd * cd + cs * cs) / (ss * ss * cd * cd);
+                    }
+                }
+            }
+            const float u_fresnel = L.glass ? u24(r.x) : u24(r.y);
+            if (u_fresnel > R) {
+                if (next == 0) {
+                    // leaves the tissue: detectors (mcml_kernel.cpp:257-268)
+                    detect_and_tally(P, S, s_det, ph);
+                    if (ph.dz < 0.0f) kill(S, ph, alive, L_N_TOP, L_TOP);
+                    else kill(S, ph, alive, L_N_BOTTOM, L_BOTTOM);
+                    continue;
+                }
+                // RefractVector (mcml_kernel.cpp:595-616)
+                const float six = ni * ph.dx, siy = ni * ph.dy, siz = ni * ph.dz;
+                const float t1 = six * nx + siy * ny + siz * nz;
+                float t2 = sqrtf((nt * nt - ni * ni) / (t1 * t1) + 1.0f);
+                t2 = (t2 - 1.0f) * t1;
+                float ox = six + t2 * nx, oy = siy + t2 * ny, oz = siz + t2 * nz;
+                const float on = rsqrtf(ox * ox + oy * oy + oz * oz);
+                ph.dx = ox * on; ph.dy = oy * on; ph.dz = oz * on;
+                ph.layer = next;
+                ph.visited |= 1u << next;
+            } else {
+                // ReflectVector (mcml_kernel.cpp:582-593)
+                const float t = 2.0f * dn;
+                float ox = ph.dx - t * nx, oy = ph.dy - t * ny, oz = ph.dz - t * nz;
+                const float on = rsqrtf(ox * ox + oy * oy + oz * oz);
+                ph.dx = ox * on; ph.dy = oy * on; ph.dz = oz * on;
+            }
+            ph.excl = hit.tri;
+            ph.tmin = kTminAfter;
+        } else {
+            // ---- drop (mcml_kernel.cpp:633-642) ----
+            uint32_t dw = __float2uint_rn(__uint2float_rn(ph.w) * L.absorb);
+            dw = min(dw, ph.w);
+            ph.w -= dw;
+            if (idx >= 0) {
+                if (dw) atomicAdd(&P.absorb[idx], (unsigned long long)dw);
+                lat(&S.ledger[L_ABSORBED], dw);
+            } else {
+                lat(&S.ledger[L_ABSORBED_OUT], dw);
+            }
+            // ---- spin (mcml_kernel.cpp:442-495) ----
+            const float u1 = u24(r.y);
+            float cost;
+            if (L.g != 0.0f) {
+                const float t = L.hg_a / (L.hg_d + L.hg_e * u1);
+                cost = (L.hg_b - t * t) * L.hg_c;
+            } else {
+                cost = 2.0f * u1 - 1.0f;
+            }
+            cost = fminf(1.0f, fmaxf(-1.0f, cost));
+            const float sint = sqrtf(fmaxf(0.0f, 1.0f - cost * cost));
+            float a = u24(r.z);
+            a = a > 0.5f ? a - 1.0f : a;  // same angle as 2*pi*u, reduced to [-pi, pi]
+            float sp, cp;
+            __sincosf(6.283185307179586f * a, &sp, &cp);
+            const float ux = ph.dx, uy = ph.dy, uz = ph.dz;
+            const float rho2 = ux * ux + uy * uy;
+            float nx, ny, nz;
+            if (rho2 > 1e-12f) {
+                const float irho = rsqrtf(rho2);
+                const float rho = rho2 * irho;
+                nx = sint * (ux * uz * cp - uy * sp) * irho + ux * cost;
+                ny = sint * (uy * uz * cp + ux * sp) * irho + uy * cost;
+                nz = -sint * cp * rho + uz * cost;
+            } else {
+                nx = sint * cp;
+                ny = sint * sp;
+                nz = uz >= 0.0f ? cost : -cost;
+            }
+            const float on = rsqrtf(nx * nx + ny * ny + nz * nz);
+            ph.dx = nx * on; ph.dy = ny * on; ph.dz = nz * on;
+            ph.excl = -1;
+            ph.tmin = 0.0f;
+        }
+        // ---- weight cut / roulette (mcml_kernel.cpp:121-124; planar GPU kernel.cu:214-222) ----
+        if (ph.w < P.w_min) {
+            if (roulette) {
+                if (ph.w == 0u) {
+                    kill(S, ph, alive, L_N_ROULETTE, L_RKILLED);
+                } else if (u_roulette < P.chance) {
+                    const uint32_t nw = min(__float2uint_rn(__uint2float_rn(ph.w) * P.inv_chance), kWeightOne);
+                    lat(&S.ledger[L_RGAINED], nw - ph.w);
+                    ph.w = nw;
+                } else {
+                    kill(S, ph, alive, L_N_ROULETTE, L_RKILLED);
+                }
+            } else {
+                kill(S, ph, alive, L_N_CUT, L_CUT);
+            }
+        }
+    }
+
+    // ---- flush block-private tallies ----
+    atomicAdd(&S.ledger[L_STEPS], (unsigned long long)steps);
+    if (retests) atomicAdd(&S.ledger[L_N_RETEST], (unsigned long long)retests);
+    atomicAdd(&S.ledger[L_N_NODES], (unsigned long long)n_visit);
+    atomicAdd(&S.ledger[L_N_TRIS], (unsigned long long)n_tri);
+    if (budget_hit) atomicOr(P.status, 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kLedgerSlots; i += blockDim.x) lat(&P.ledger[i], s_ledger[i]);
+    for (int i = threadIdx.x; i < 4 * P.n_dets; i += blockDim.x) lat(&P.det[i], s_dettal[i]);
+}
+
+__global__ void philox_probe_kernel(uint32_t k0, uint32_t k1, unsigned long long pid, uint32_t n, uint4* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), i, 0u), k0, k1);
+}
+
+cudaError_t enqueue_transport(Context* ctx) {
+    transport_kernel<<<ctx->grid, ctx->block, ctx->smem_bytes, ctx->stream>>>(ctx->kp);
+    return cudaGetLastError();
+}
+
+cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel, block, smem);
+}
+
+cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n, uint32_t* host_out) {
+    uint4* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(uint4) * (size_t)(n ? n : 1));
+    if (e != cudaSuccess) return e;
+    philox_probe_kernel<<<(n + 127) / 128, 128>>>(key0, key1, pid, n, d);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(host_out, d, sizeof(uint4) * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e;
+}
+
+}  // namespace xmc
+
+// Host run of the kernel's ray query on the geometry image of `in` (self-test of the traversal).
+extern "C" int xmc_debug_nearest(const InputInfo* in, int n_rays, const float* rays, float tmin, float tmax,
+                                 float* t_out, int* surf_out, float* normal_out) {
+    xmc::GeomImage g;
+    std::string err;
+    if (!xmc::build_geometry(in, &g, &err)) { xmc::set_error(err); return XMC_ERR_INVALID_INPUT; }
+    for (int r = 0; r < n_rays; ++r) {
+        const float* q = rays + 6 * (size_t)r;
+        unsigned retests = 0, nv = 0, nt = 0;
+        xmc::Hit h = xmc::bvh_nearest(g.nodes.data(), g.tris.data(), g.n_nodes, nullptr, 0, nullptr, 0, q[0], q[1], q[2],
+                                      q[3], q[4], q[5], tmin, tmax, -1, retests, nv, nt);
+        t_out[r] = h.tri >= 0 ? h.t : INFINITY;
+        surf_out[r] = h.tri >= 0 ? xmc::f2i(g.tris[3 * (size_t)h.tri].w) : -1;
+        if (normal_out && h.tri >= 0) {
+            const float4 a = g.tris[3 * (size_t)h.tri], b = g.tris[3 * (size_t)h.tri + 1], c = g.tris[3 * (size_t)h.tri + 2];
+            const float e1x = a.x - b.x, e1y = a.y - b.y, e1z = a.z - b.z, e2x = a.x - c.x, e2y = a.y - c.y, e2z = a.z - c.z;
+            float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+            const float nr = 1.0f / sqrtf(nx * nx + ny * ny + nz * nz);
+            normal_out[3 * (size_t)r] = nx * nr; normal_out[3 * (size_t)r + 1] = ny * nr; normal_out[3 * (size_t)r + 2] = nz * nr;
+        }
+    }
+    return XMC_OK;
+}

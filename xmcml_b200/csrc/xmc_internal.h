@@ -1,0 +1,160 @@
+// Internal declarations shared by the host C++ files and the CUDA transport kernel.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+// CUDA's vector_types.h also defines double3 and int3; inside this library the reference's
+// vertex and index types are named xmc_ref_double3 / xmc_ref_int3 (same layout, same union tags).
+#define double3 xmc_ref_double3
+#define int3 xmc_ref_int3
+#include "../../include/xmcml_b200.h"
+#undef double3
+#undef int3
+
+namespace xmc {
+
+// Fixed point of photon weights and tallies: weight 1.0 == 2^31.
+constexpr double kWeightScale = 2147483648.0;
+constexpr uint32_t kWeightOne = 0x80000000u;
+
+// Geometric tolerances of the FP32 walk (mm). A step that ends within kStepExtend in front of a
+// surface is taken to the surface; after a boundary interaction hits closer than kTminAfter are
+// ignored and the triangle just hit is excluded from the next query. The reference's FP64 nudges
+// of 1e-8 mm (mcml_kernel.cpp:13) are below FP32 resolution at mm scale and are replaced by these.
+constexpr float kStepExtend = 2e-6f;
+constexpr float kTminAfter = 2e-6f;
+// Band around triangle edges inside which the FP32 ray-triangle test is redone in FP64: about
+// kEdgeBandLength mm measured along the triangle, as a barycentric width clamped to
+// [kEdgeBandMin, kEdgeBandMax] (FP32 barycentrics carry ~1e-7 relative error).
+constexpr float kEdgeBandLength = 1e-5f;
+constexpr float kEdgeBandMin = 1.0f / 262144.0f;
+constexpr float kEdgeBandMax = 1.0f / 1024.0f;
+
+// Per-layer constants of the walk (FP32).
+struct DevLayer {
+    float n;          // refractive index
+    float mua, mus;   // mm^-1
+    float g;          // anisotropy
+    float inv_mut;    // 1 / (mua + mus), 0 for glass
+    float absorb;     // mua / (mua + mus)
+    float hg_a;       // 1 - g^2
+    float hg_b;       // 1 + g^2
+    float hg_c;       // 1 / (2 g)  (0 when g == 0)
+    float hg_d;       // 1 - g
+    float hg_e;       // 2 g
+    int glass;        // 1 when mua == mus == 0
+};
+
+// Detector record: cube detectors first, then rings (the reference's GetDetectorId order).
+struct DevDetector {
+    float cx, cy, cz;     // centre
+    float hx, hy, hz;     // cube: half lengths; ring: (small radius, big radius, unused)
+    float cos_angle;      // cos(targetAngle) as computed by the reference, rounded to float
+    uint32_t filter;      // bitmask of filterLayers
+};
+
+// Ledger slots of the device tally (uint64 each).
+enum LedgerSlot {
+    L_LAUNCHED = 0, L_TERMINATED, L_STEPS,
+    L_N_TOP, L_N_BOTTOM, L_N_AREA, L_N_CUT, L_N_ROULETTE, L_N_GLASS, L_N_BUDGET, L_N_INVALID,
+    L_N_DETECTED, L_N_RETEST, L_N_NODES, L_N_TRIS,
+    L_ABSORBED, L_ABSORBED_OUT, L_TOP, L_BOTTOM, L_AREA, L_CUT, L_GLASS, L_BUDGET, L_INVALID,
+    L_RKILLED, L_RGAINED,
+    L_COUNT
+};
+constexpr int kLedgerSlots = 32;  // padded
+
+// Everything the kernel reads, by value (kernel parameter space).
+struct KParams {
+    // geometry
+    const float4* nodes;      // 2 float4 per node
+    const float4* tris;       // 3 float4 per triangle
+    const int8_t* next_layer; // [n_surf * MAX_LAYERS]: layer across surface s from layer l, -1 if none
+    int n_nodes, n_tris, n_surf;
+    int smem_nodes, smem_tris, smem_next;  // how many of each are staged in shared memory
+    // layers
+    DevLayer layer[MAX_LAYERS];
+    int n_layers;
+    uint32_t target_mask;     // targetRangeLayers as bitmask
+    // Area
+    float ax, ay, az;         // corner
+    float asx, asy, asz;      // partitions / length
+    int nx, ny, nz;
+    int byte_sentinel;        // voxel (255,255,255) counts as outside (reference byte index semantics)
+    // detectors and time bins
+    const DevDetector* dets;
+    int n_cubes, n_rings, n_dets;
+    float t0, dt;             // time bins: [t0 + i dt, t0 + (i+1) dt), last bin open-ended
+    int n_time;
+    // launch
+    float sx, sy, sz, dx, dy, dz;
+    float beam_radius;
+    uint32_t w0;              // start weight (fixed point)
+    uint32_t w_min;           // minWeight (fixed point)
+    float chance, inv_chance; // roulette
+    uint32_t flags;
+    uint32_t key0, key1;      // Philox key (seed)
+    unsigned long long first_id, n_photons, max_steps;
+    int chunk;
+    // tallies (device, fixed point)
+    unsigned long long* absorb;   // [nx*ny*nz]
+    unsigned long long* det;      // [n_dets * 4]: weight, count, target weight, weight^2
+    unsigned long long* tbin;     // [n_dets * n_time * 4]
+    unsigned long long* ledger;   // [kLedgerSlots]
+    unsigned long long* counter;  // photon id dispenser
+    const volatile int* cancel;   // host-mapped cancel flag (may be null)
+    int* status;                  // device status word: bit0 budget hit, bit1 cancelled
+};
+
+// Host-side device image and buffers of one context.
+struct Context {
+    int device = 0;
+    xmc_options opt{};
+    KParams kp{};
+    double rsp = 0.0;         // specular reflectance (FP64, as the reference computes it)
+    uint32_t w0_fx = 0;
+    int grid_size = 0, n_dets = 0, n_time = 0;
+    size_t smem_bytes = 0;
+    int block = 256, blocks_per_sm = 0, num_sms = 0, grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // device buffers
+    void* d_nodes = nullptr; void* d_tris = nullptr; void* d_next = nullptr; void* d_dets = nullptr;
+    void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
+    void* d_counter = nullptr; void* d_status = nullptr;
+    int* h_cancel = nullptr;  // pinned, mapped
+    // pinned read-back buffers
+    unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;
+    unsigned long long* h_tbin = nullptr; unsigned long long* h_ledger = nullptr;
+    int* h_status = nullptr;
+    // time bin edges of the reference (FP64), for OutputInfo
+    std::vector<double> bin_start, bin_finish;
+    uint64_t last_n = 0;
+    double last_kernel_ms = 0.0, last_total_ms = 0.0;
+    uint64_t h2d_bytes = 0;   // bytes uploaded by xmc_create (device image)
+};
+
+// Host image of the geometry before upload.
+struct GeomImage {
+    std::vector<float4> nodes;   // 2 per node
+    std::vector<float4> tris;    // 3 per triangle
+    int n_nodes = 0, n_tris = 0;
+};
+
+// bvh.cpp
+bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err);
+
+// transport.cu: enqueue one transport kernel launch on ctx->stream (tallies must be zeroed).
+cudaError_t enqueue_transport(Context* ctx);
+// transport.cu: occupancy of the kernel for a block size and dynamic shared memory.
+cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm);
+// transport.cu: Philox blocks computed on the device (self test).
+cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n, uint32_t* host_out);
+
+void set_error(const std::string& msg);
+
+}  // namespace xmc

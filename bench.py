@@ -108,23 +108,33 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def _ref_sample_size(info, seconds, threads):
+    """Photon count for about `seconds` of the reference's LaunchOMP, from growing probe runs."""
+    from oracle import bind as OB
+    n = max(threads * 50, 500)
+    while True:
+        out = OB.ref_new_output(info, fast=True)
+        t0 = time.perf_counter()
+        OB.ref_launch(info, out, 5, threads, fast=True, n=n)
+        dt = time.perf_counter() - t0
+        OB.ref(True).ref_free_output(C.byref(out))
+        if dt > min(2.0, seconds / 4) or n > 5e7:
+            return int(max(threads * 50, min(n / dt * seconds, 5e7)))
+        n *= 4
+
+
 def cpu_reference_rate(xml, surf, seconds, threads, seed=777):
     """The reference's LaunchOMP (oracle/_ref/libxmcml_ref_fast.so, -O3, all threads) on a bounded
-    sample of the workload; returns (photons/s, photons, seconds, threads)."""
+    sample of the workload; returns (photons/s, photons, seconds)."""
     from oracle import bind as OB
     info = OB.ref_load_model(xml, surf, fast=True)
     OB.ref(True).ref_generate_bvh(C.byref(info))  # prebuilt tree, outside the timed region
-    out = OB.ref_new_output(info, fast=True)
-    n = max(threads * 50, 500)
-    t0 = time.perf_counter()
-    OB.ref_launch(info, out, seed, threads, fast=True, n=n)
-    dt = time.perf_counter() - t0
-    rate = n / dt
-    n2 = int(max(threads * 100, min(rate * seconds, 5e7)))
+    n2 = _ref_sample_size(info, seconds, threads)
     out2 = OB.ref_new_output(info, fast=True)
     t0 = time.perf_counter()
     OB.ref_launch(info, out2, seed + 1, threads, fast=True, n=n2)
     dt = time.perf_counter() - t0
+    OB.ref(True).ref_free_output(C.byref(out2))
     return n2 / dt, n2, dt
 
 
@@ -142,15 +152,12 @@ def run_reference_arm(args, rank, world):
     threads = os.cpu_count() or 1
     info = OB.ref_load_model(xml, surf, fast=True)
     OB.ref(True).ref_generate_bvh(C.byref(info))
-    # size one step at about 8 s of work from a probe run
+    # size one step at about 8 s of work from growing probe runs
+    n_step = _ref_sample_size(info, 8.0, threads)
     out = OB.ref_new_output(info, fast=True)
-    n = max(threads * 50, 500)
-    t0 = time.perf_counter()
-    OB.ref_launch(info, out, 1, threads, fast=True, n=n)
-    rate0 = n / (time.perf_counter() - t0)
-    n_step = int(max(threads * 50, min(rate0 * 8.0, 5e7)))
     for w in range(args.warmup):
-        OB.ref_launch(info, out, 100 + w, threads, fast=True, n=max(n_step // 4, threads * 10))
+        OB.ref_launch(info, out, 100 + w, threads, fast=True, n=max(n_step // 8, threads * 10))
+    OB.ref(True).ref_free_output(C.byref(out))
     times = []
     for k in range(args.steps):
         out = OB.ref_new_output(info, fast=True)
@@ -171,6 +178,43 @@ def run_reference_arm(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
+
+def run_e2e(args, m, N, rank, local, world, barrier, dist, torch):
+    """e2e photons/s through xmc_launch_omp with host InputInfo/OutputInfo (see module docstring)."""
+    from xmcml_b200 import api, _lib
+    lib = _lib.load()
+    tree = lib.xmc_generate_bvh_tree(m.info.surface, m.info.numberOfSurfaces)  # prebuilt once, like the reference launcher
+    m.info.bvhTree = tree
+    m.info.numberOfPhotons = N
+    probe = api.Transport(m, roulette=False, device=local)
+    pled = probe.run(1000, seed=1)
+    probe.close()
+    h2d = pled["h2d_bytes"]
+    out = api.Output(m)
+    rng = api.mcg59_init(777 + rank, 0, 1)
+    api.launch_omp(m, out, rng, 0)  # warm
+    barrier()
+    e2e_t = []
+    for k in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        api.launch_omp(m, out, rng, 0)
+        e2e_t.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = sum(e2e_t)
+    if dist is not None:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = tt.item()
+    e2e_value = world * args.e2e_steps * N / e2e_s
+    grid = out.info.gridSize
+    D = out.info.numberOfDetectors
+    T = m.info.timeScaleSize
+    d2h = 8 * grid + 32 * D + 32 * D * T + 8 * 32 + 16
+    m.info.bvhTree = None
+    lib.xmc_free_bvh_tree(tree)
+
+    return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "via": "xmc_launch_omp (LaunchOMP signature), host InputInfo/OutputInfo"}
 
 def roofline(led, kernel_ms, clocks, n_photons):
     """Issue-bound roofline of the transport kernel from the per-step cost model (48 FP32 flop,
@@ -251,36 +295,10 @@ def main():
     last = leds[-1]
 
     # ---- e2e through the reference-signature C-ABI with host buffers ----
-    lib = _lib.load()
-    tree = lib.xmc_generate_bvh_tree(m.info.surface, m.info.numberOfSurfaces)  # prebuilt once, like the reference launcher
-    m.info.bvhTree = tree
-    m.info.numberOfPhotons = N
-    probe = api.Transport(m, roulette=False, device=local)
-    pled = probe.run(1000, seed=1)
-    probe.close()
-    h2d = pled["h2d_bytes"]
-    out = api.Output(m)
-    rng = api.mcg59_init(777 + rank, 0, 1)
-    api.launch_omp(m, out, rng, 0)  # warm
-    barrier()
-    e2e_t = []
-    for k in range(args.e2e_steps):
-        t0 = time.perf_counter()
-        api.launch_omp(m, out, rng, 0)
-        e2e_t.append(time.perf_counter() - t0)
-    barrier()
-    e2e_s = sum(e2e_t)
-    if dist is not None:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = tt.item()
-    e2e_value = world * args.e2e_steps * N / e2e_s
-    grid = out.info.gridSize
-    D = out.info.numberOfDetectors
-    T = m.info.timeScaleSize
-    d2h = 8 * grid + 32 * D + 32 * D * T + 8 * 32 + 16
-    m.info.bvhTree = None
-    lib.xmc_free_bvh_tree(tree)
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e = run_e2e(args, m, N, rank, local, world, barrier, dist, torch)
+    line_e2e = e2e
 
     rl = roofline(last, last["kernel_ms"], clocks, N)
     prof = os.path.join(ROOT, "profiles", f"transport_kernel_{args.workload}_dram.json")
@@ -312,8 +330,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "config": cfg, "clocks": clocks,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "via": "xmc_launch_omp (LaunchOMP signature), host InputInfo/OutputInfo"},
+            "e2e": line_e2e,
             "gpu_launches": args.steps, "roofline": rl, "cpu_baseline": cpu,
             "kernel_ms_per_step": ker_ms / args.steps,
             "walk": {"steps_per_photon": last["steps"] / N, "detected_fraction": last["n_detected"] / N,

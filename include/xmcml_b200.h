@@ -223,7 +223,7 @@ typedef struct xmc_options {
     int32_t  device;               /* CUDA device ordinal (default 0)                            */
     int32_t  block_size;           /* threads per block (0 = autotuned / default 256)             */
     int32_t  blocks_per_sm;        /* resident blocks per SM (0 = occupancy maximum)              */
-    int32_t  photons_per_chunk;    /* photon ids a warp claims at a time (0 = 256)                */
+    int32_t  photons_per_chunk;    /* photon ids a warp claims at a time (0 = 64)                 */
     int32_t  smem_nodes;           /* BVH nodes staged in shared memory (-1 = none, 0 = auto)      */
     int32_t  reserved[7];
 } xmc_options;

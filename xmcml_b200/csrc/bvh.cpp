@@ -329,6 +329,34 @@ bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err) {
     return true;
 }
 
+int occupied_z_slabs(const GeomImage& g, float* lo, float* hi) {
+    std::vector<std::pair<float, float>> iv;
+    iv.reserve(g.n_tris);
+    for (int i = 0; i < g.n_tris; ++i) {
+        const float4 a = g.tris[3 * (size_t)i], b = g.tris[3 * (size_t)i + 1], c = g.tris[3 * (size_t)i + 2];
+        float zl = std::min(a.z, std::min(b.z, c.z)), zh = std::max(a.z, std::max(b.z, c.z));
+        const float pad = 1e-5f * std::max(1.0f, std::max(std::fabs(zl), std::fabs(zh)));
+        iv.push_back({zl - pad, zh + pad});
+    }
+    std::sort(iv.begin(), iv.end());
+    std::vector<std::pair<float, float>> m;
+    for (auto& v : iv) {
+        if (!m.empty() && v.first <= m.back().second) m.back().second = std::max(m.back().second, v.second);
+        else m.push_back(v);
+    }
+    // too many: close the narrowest gaps (a larger occupied set is still correct)
+    while ((int)m.size() > kMaxZSlabs) {
+        size_t best = 0;
+        float gap = INFINITY;
+        for (size_t i = 0; i + 1 < m.size(); ++i)
+            if (m[i + 1].first - m[i].second < gap) { gap = m[i + 1].first - m[i].second; best = i; }
+        m[best].second = std::max(m[best].second, m[best + 1].second);
+        m.erase(m.begin() + best + 1);
+    }
+    for (size_t i = 0; i < m.size(); ++i) { lo[i] = m[i].first; hi[i] = m[i].second; }
+    return (int)m.size();
+}
+
 // GenerateBVHTree replacement (mcml_intersection.cpp:316-344): a binned-SAH tree of this library
 // returned in the reference's own BVHTree layout (FP64 boxes, leaves as (surfId, trIndex) runs,
 // nodes listed children-before-parent with the root last, as the reference emits them), so callers

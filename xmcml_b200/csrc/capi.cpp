@@ -121,7 +121,7 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
         opt.struct_size = sizeof(xmc_options);
         if (opt.roulette_chance == 0) opt.roulette_chance = 0.1;
         if (opt.max_steps_per_photon == 0) opt.max_steps_per_photon = 10000000ull;
-        if (opt.photons_per_chunk <= 0) opt.photons_per_chunk = 256;
+        if (opt.photons_per_chunk <= 0) opt.photons_per_chunk = 64;
     }
     int st = validate(in, opt);
     if (st) return st;
@@ -278,6 +278,7 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.smem_next = smem_next;
     kp.n_nodes = geom.n_nodes;
     kp.n_tris = geom.n_tris;
+    kp.n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
     c->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next);
 
     // ---- device buffers ----
@@ -468,7 +469,7 @@ void xmc_default_options(xmc_options* o) {
     o->struct_size = sizeof(xmc_options);
     o->roulette_chance = 0.1;
     o->max_steps_per_photon = 10000000ull;
-    o->photons_per_chunk = 256;
+    o->photons_per_chunk = 64;
 }
 
 int xmc_create(const InputInfo* input, const xmc_options* opt, xmc_context** out_ctx) {

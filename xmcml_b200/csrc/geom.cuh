@@ -31,6 +31,25 @@ struct Hit {
     int tri;  // index into the triangle array, -1 if none
 };
 
+// FP64 re-test of a ray-triangle pair near an edge (rare; kept out of line to spare registers).
+__host__ __device__ __noinline__ float tri_distance_fp64(float4 a, float4 b, float4 c, float ox, float oy, float oz,
+                                                        float dx, float dy, float dz) {
+    const double E1x = (double)b.x - a.x, E1y = (double)b.y - a.y, E1z = (double)b.z - a.z;
+    const double E2x = (double)c.x - a.x, E2y = (double)c.y - a.y, E2z = (double)c.z - a.z;
+    const double Dx = dx, Dy = dy, Dz = dz;
+    const double Px = Dy * E2z - Dz * E2y, Py = Dz * E2x - Dx * E2z, Pz = Dx * E2y - Dy * E2x;
+    const double Det = E1x * Px + E1y * Py + E1z * Pz;
+    if (Det < 1e-6 && Det > -1e-6) return INFINITY;
+    const double Inv = 1.0 / Det;
+    const double Sx = (double)ox - a.x, Sy = (double)oy - a.y, Sz = (double)oz - a.z;
+    const double U = (Sx * Px + Sy * Py + Sz * Pz) * Inv;
+    if (U < 0.0 || U > 1.0) return INFINITY;
+    const double Qx = Sy * E1z - Sz * E1y, Qy = Sz * E1x - Sx * E1z, Qz = Sx * E1y - Sy * E1x;
+    const double V = (Dx * Qx + Dy * Qy + Dz * Qz) * Inv;
+    if (V < 0.0 || U + V > 1.0) return INFINITY;
+    return (float)((E2x * Qx + E2y * Qy + E2z * Qz) * Inv);
+}
+
 // Moller-Trumbore in FP32 with the reference's determinant cut (mcml_intersection.cpp:44-86).
 // Inside a barycentric band around the edges (width stored per triangle in c.w: kEdgeBandLength
 // divided by the triangle's shortest edge, at least kEdgeBandMin) the test is redone in FP64 on the
@@ -51,24 +70,9 @@ __host__ __device__ __forceinline__ float tri_distance(float4 a, float4 b, float
     const float band = c.w;  // per-triangle barycentric width of the FP64 re-test band
     if (u < -band || v < -band || w < -band) return INFINITY;
     if (u > band && v > band && w > band) return (e2x * qx + e2y * qy + e2z * qz) * inv;
-    // FP64 re-test in the edge band.
     ++retests;
-    const double E1x = (double)b.x - a.x, E1y = (double)b.y - a.y, E1z = (double)b.z - a.z;
-    const double E2x = (double)c.x - a.x, E2y = (double)c.y - a.y, E2z = (double)c.z - a.z;
-    const double Dx = dx, Dy = dy, Dz = dz;
-    const double Px = Dy * E2z - Dz * E2y, Py = Dz * E2x - Dx * E2z, Pz = Dx * E2y - Dy * E2x;
-    const double Det = E1x * Px + E1y * Py + E1z * Pz;
-    if (Det < 1e-6 && Det > -1e-6) return INFINITY;
-    const double Inv = 1.0 / Det;
-    const double Sx = (double)ox - a.x, Sy = (double)oy - a.y, Sz = (double)oz - a.z;
-    const double U = (Sx * Px + Sy * Py + Sz * Pz) * Inv;
-    if (U < 0.0 || U > 1.0) return INFINITY;
-    const double Qx = Sy * E1z - Sz * E1y, Qy = Sz * E1x - Sx * E1z, Qz = Sx * E1y - Sy * E1x;
-    const double V = (Dx * Qx + Dy * Qy + Dz * Qz) * Inv;
-    if (V < 0.0 || U + V > 1.0) return INFINITY;
-    return (float)((E2x * Qx + E2y * Qy + E2z * Qz) * Inv);
+    return tri_distance_fp64(a, b, c, ox, oy, oz, dx, dy, dz);
 }
-
 // Nearest hit with tmin <= t <= tmax over the threaded BVH (no stack): the reference's
 // ComputeBVHIntersection / ComputeBVHIntersectionWithoutStep contract (mcml_intersection.cpp:354-584).
 // Nodes below n_smem_nodes and triangles below n_smem_tris are read from the staged copies.

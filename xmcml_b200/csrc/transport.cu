@@ -50,8 +50,26 @@ struct Photon {
     uint32_t iter;
     int excl;
     float tmin;
+    float gap_lo, gap_hi;  // triangle-free z-gap containing the photon (empty if none)
     unsigned long long pid;
 };
+
+// The triangle-free z-gap around z: (highest occupied top below z, lowest occupied bottom above
+// z), or an empty interval when z lies inside an occupied slab.
+__device__ __forceinline__ void find_gap(const float* __restrict__ zlo, const float* __restrict__ zhi, int n, float z,
+                                         float& glo, float& ghi) {
+    glo = -INFINITY;
+    ghi = INFINITY;
+    for (int i = 0; i < n; ++i) {
+        if (z >= zlo[i] && z <= zhi[i]) {
+            glo = INFINITY;
+            ghi = -INFINITY;
+            return;
+        }
+        if (zhi[i] < z) glo = fmaxf(glo, zhi[i]);
+        if (zlo[i] > z) ghi = fminf(ghi, zlo[i]);
+    }
+}
 
 // GetAreaIndex (mcml_kernel.cpp:190-227): voxel of a point, -1 outside Area. `tol` (voxel units)
 // widens the box for points on a surface: the reference stops 1e-10 mm in front of a surface
@@ -162,7 +180,7 @@ __device__ __forceinline__ void launch_photon(const KParams& P, Photon& ph, unsi
 
 }  // namespace
 
-__global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
+__global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     // --- shared memory carve-up (must match smem_layout on the host) ---
     unsigned long long* s_ledger = reinterpret_cast<unsigned long long*>(smem);
@@ -172,6 +190,11 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
     DevLayer* s_layer = reinterpret_cast<DevLayer*>(s_tris + 3 * P.smem_tris);
     DevDetector* s_det = reinterpret_cast<DevDetector*>(s_layer + MAX_LAYERS);
     int8_t* s_next = reinterpret_cast<int8_t*>(s_det + P.n_dets);
+    __shared__ float s_zlo[kMaxZSlabs], s_zhi[kMaxZSlabs];
+    for (int i = threadIdx.x; i < P.n_zocc; i += blockDim.x) {
+        s_zlo[i] = P.zocc_lo[i];
+        s_zhi[i] = P.zocc_hi[i];
+    }
 
     for (int i = threadIdx.x; i < kLedgerSlots + 4 * P.n_dets; i += blockDim.x) s_ledger[i] = 0ull;
     for (int i = threadIdx.x; i < 2 * P.smem_nodes; i += blockDim.x) s_nodes[i] = __ldg(&P.nodes[i]);
@@ -192,6 +215,7 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
     bool alive = false;
     Photon ph;
     unsigned steps = 0, retests = 0, n_visit = 0, n_tri = 0;
+    unsigned long long absorbed = 0, absorbed_out = 0;  // per-thread sums, flushed once at the end
     unsigned budget_hit = 0;
 
     for (;;) {
@@ -221,6 +245,7 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
             const int take = (int)min((unsigned long long)cnt, avail);
             if (((need >> lane) & 1u) && rank < take) {
                 launch_photon(P, ph, P.first_id + cbeg + rank);
+                find_gap(s_zlo, s_zhi, P.n_zocc, ph.pz, ph.gap_lo, ph.gap_hi);
                 alive = true;
                 atomicAdd(&S.ledger[L_LAUNCHED], 1ull);
             }
@@ -239,7 +264,7 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
         const uint4 r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter, 0u), P.key0, P.key1);
         ph.iter++;
         steps++;
-        const DevLayer L = s_layer[ph.layer];
+        const DevLayer& L = s_layer[ph.layer];
         float u_roulette;
         bool boundary;
         Hit hit;
@@ -256,8 +281,14 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
             step = hit.t;
         } else {
             step = -__logf(u24(r.x)) * L.inv_mut;  // mcml_kernel.cpp:618-631
-            hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py, ph.pz,
-                              ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
+            const float zend = fmaf(step + kStepExtend, ph.dz, ph.pz);
+            if (fminf(ph.pz, zend) > ph.gap_lo && fmaxf(ph.pz, zend) < ph.gap_hi) {
+                hit.tri = -1;  // the step stays inside a triangle-free z-gap: no surface to cross
+                hit.t = step;
+            } else {
+                hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
+                                  ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
+            }
             boundary = hit.tri >= 0;
             if (boundary) step = hit.t;
             u_roulette = boundary ? u24(r.z) : u24(r.w);
@@ -267,6 +298,7 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
         ph.py = fmaf(step, ph.dy, ph.py);
         ph.pz = fmaf(step, ph.dz, ph.pz);
         ph.time = fmaf(step, L.n, ph.time);
+        if (!(ph.pz > ph.gap_lo && ph.pz < ph.gap_hi)) find_gap(s_zlo, s_zhi, P.n_zocc, ph.pz, ph.gap_lo, ph.gap_hi);
         if ((P.target_mask >> ph.layer) & 1u) ph.trange += step;
         else ph.orange += step;
         const int idx = area_index(P, ph.px, ph.py, ph.pz, boundary ? 1e-4f : 0.0f);
@@ -370,9 +402,9 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
             ph.w -= dw;
             if (idx >= 0) {
                 if (dw) atomicAdd(&P.absorb[idx], (unsigned long long)dw);
-                lat(&S.ledger[L_ABSORBED], dw);
+                absorbed += dw;
             } else {
-                lat(&S.ledger[L_ABSORBED_OUT], dw);
+                absorbed_out += dw;
             }
             // ---- spin (mcml_kernel.cpp:442-495) ----
             const float u1 = u24(r.y);
@@ -428,6 +460,8 @@ __global__ void __launch_bounds__(256, 2) transport_kernel(const KParams P) {
 
     // ---- flush block-private tallies ----
     atomicAdd(&S.ledger[L_STEPS], (unsigned long long)steps);
+    lat(&S.ledger[L_ABSORBED], absorbed);
+    lat(&S.ledger[L_ABSORBED_OUT], absorbed_out);
     if (retests) atomicAdd(&S.ledger[L_N_RETEST], (unsigned long long)retests);
     atomicAdd(&S.ledger[L_N_NODES], (unsigned long long)n_visit);
     atomicAdd(&S.ledger[L_N_TRIS], (unsigned long long)n_tri);
@@ -448,7 +482,14 @@ cudaError_t enqueue_transport(Context* ctx) {
 }
 
 cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm) {
-    cudaError_t e = cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, transport_kernel);
+    if (e != cudaSuccess) return e;
+    if (block > fa.maxThreadsPerBlock) {
+        *blocks_per_sm = 0;
+        return cudaSuccess;
+    }
+    e = cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel, block, smem);
 }

@@ -68,6 +68,10 @@ enum LedgerSlot {
 };
 constexpr int kLedgerSlots = 32;  // padded
 
+// z-intervals occupied by triangles (merged, padded, sorted): a step whose z-range lies strictly
+// inside a gap between them cannot cross any surface, so its ray query is skipped.
+constexpr int kMaxZSlabs = 24;
+
 // Everything the kernel reads, by value (kernel parameter space).
 struct KParams {
     // geometry
@@ -76,6 +80,8 @@ struct KParams {
     const int8_t* next_layer; // [n_surf * MAX_LAYERS]: layer across surface s from layer l, -1 if none
     int n_nodes, n_tris, n_surf;
     int smem_nodes, smem_tris, smem_next;  // how many of each are staged in shared memory
+    float zocc_lo[kMaxZSlabs], zocc_hi[kMaxZSlabs];
+    int n_zocc;
     // layers
     DevLayer layer[MAX_LAYERS];
     int n_layers;
@@ -147,6 +153,8 @@ struct GeomImage {
 
 // bvh.cpp
 bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err);
+// bvh.cpp: merged z-intervals occupied by the triangles of `g` (at most kMaxZSlabs, conservative)
+int occupied_z_slabs(const GeomImage& g, float* lo, float* hi);
 
 // transport.cu: enqueue one transport kernel launch on ctx->stream (tallies must be zeroed).
 cudaError_t enqueue_transport(Context* ctx);

@@ -111,8 +111,7 @@ static int validate(const InputInfo* in, const xmc_options& opt) {
     return XMC_OK;
 }
 
-static int create(const InputInfo* in, const xmc_options* opt_in, Context** out) {
-    *out = nullptr;
+int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img) {
     xmc_options opt;
     xmc_default_options(&opt);
     if (opt_in && opt_in->struct_size) {
@@ -125,27 +124,13 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     }
     int st = validate(in, opt);
     if (st) return st;
+    img->opt = opt;
 
-    GeomImage geom;
     std::string err;
-    if (!build_geometry(in, &geom, &err)) return fail(XMC_ERR_INVALID_INPUT, err);
+    if (!build_geometry(in, &img->geom, &err)) return fail(XMC_ERR_INVALID_INPUT, err);
+    const GeomImage& geom = img->geom;
 
-    Context* c = new (std::nothrow) Context();
-    if (!c) return fail(XMC_ERR_DEVICE, "out of host memory");
-    c->opt = opt;
-    c->device = opt.device;
-    auto bail = [&](int s) { free_context(c); return s; };
-    {
-        cudaError_t e = cudaSetDevice(c->device);
-        if (e != cudaSuccess) return bail(fail(XMC_ERR_DEVICE, std::string("cudaSetDevice: ") + cudaGetErrorString(e)));
-    }
-#define CK(call)                                                                                       \
-    do {                                                                                               \
-        cudaError_t e_ = (call);                                                                       \
-        if (e_ != cudaSuccess) return bail(fail(XMC_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_))); \
-    } while (0)
-
-    KParams& kp = c->kp;
+    KParams& kp = img->kp;
     std::memset(&kp, 0, sizeof(kp));
     // ---- layers ----
     kp.n_layers = in->numberOfLayers;
@@ -174,7 +159,8 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
         if (in->targetRangeLayers[l]) kp.target_mask |= 1u << l;
     // ---- surface -> layer transitions: FindIntersectionLayer (mcml_kernel.cpp:566-580) ----
     const int ns = in->numberOfSurfaces;
-    std::vector<int8_t> next((size_t)std::max(1, ns) * MAX_LAYERS, (int8_t)-1);
+    std::vector<int8_t>& next = img->next;
+    next.assign((size_t)std::max(1, ns) * MAX_LAYERS, (int8_t)-1);
     for (int s = 0; s < ns; ++s)
         for (int cur = 0; cur < MAX_LAYERS; ++cur) {
             int found = -1;
@@ -193,10 +179,11 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.nx = A.partitionNumber.x; kp.ny = A.partitionNumber.y; kp.nz = A.partitionNumber.z;
     kp.byte_sentinel = (A.partitionNumber.x >= 256 && A.partitionNumber.y >= 256 && A.partitionNumber.z >= 256 &&
                         !(opt.flags & XMC_LARGE_GRID)) ? 1 : 0;
-    c->grid_size = A.partitionNumber.x * A.partitionNumber.y * A.partitionNumber.z;
+    img->grid_size = A.partitionNumber.x * A.partitionNumber.y * A.partitionNumber.z;
     // ---- detectors: cubes then rings (GetDetectorId order, mcml_kernel.cpp:663-742) ----
     const int nd = in->numberOfCubeDetectors + in->numberOfRingDetectors;
-    std::vector<DevDetector> dets((size_t)std::max(1, nd));
+    std::vector<DevDetector>& dets = img->dets;
+    dets.assign((size_t)std::max(1, nd), DevDetector{});
     const double kPi = 3.14159265358979323846;
     for (int i = 0; i < in->numberOfCubeDetectors; ++i) {
         const CubeDetector& D = in->cubeDetector[i];
@@ -219,28 +206,20 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.n_cubes = in->numberOfCubeDetectors;
     kp.n_rings = in->numberOfRingDetectors;
     kp.n_dets = nd;
-    c->n_dets = nd;
+    img->n_dets = nd;
     // ---- time bins: InitOutput (launcher_omp.cpp:36-55) ----
     const int T = in->timeScaleSize;
     double tstep = (in->timeFinish - in->timeStart) / T;
     if (tstep < 0.0) tstep = 0.0;
-    c->bin_start.resize(T);
-    c->bin_finish.resize(T);
-    for (int j = 0; j < T - 1; ++j) {
-        c->bin_start[j] = in->timeStart + j * tstep;
-        c->bin_finish[j] = c->bin_start[j] + tstep;
-    }
-    c->bin_start[T - 1] = in->timeStart + (T - 1) * tstep;
-    c->bin_finish[T - 1] = in->timeFinish;
     kp.t0 = (float)in->timeStart;
     kp.dt = (float)tstep;
     kp.n_time = T;
-    c->n_time = T;
+    img->n_time = T;
     // ---- launch (mcml_kernel.cpp:128-149) ----
-    c->rsp = specular(in->layerInfo);
-    const double w0 = 1.0 - c->rsp;
-    c->w0_fx = (uint32_t)std::llround(w0 * kWeightScale);
-    kp.w0 = c->w0_fx;
+    img->rsp = specular(in->layerInfo);
+    const double w0 = 1.0 - img->rsp;
+    img->w0_fx = (uint32_t)std::llround(w0 * kWeightScale);
+    kp.w0 = img->w0_fx;
     {
         double wm = std::ceil(in->minWeight * kWeightScale);
         if (!(wm > 0)) wm = 0;
@@ -261,9 +240,6 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.chunk = opt.photons_per_chunk;
 
     // ---- shared-memory staging plan ----
-    cudaDeviceProp prop;
-    CK(cudaGetDeviceProperties(&prop, c->device));
-    c->num_sms = prop.multiProcessorCount;
     const size_t smem_cap = 48 * 1024;  // per block, leaves room for several blocks per SM
     int smem_next = (int)std::min<size_t>((size_t)ns * MAX_LAYERS, 4096);
     int smem_tris = geom.n_tris <= 256 ? geom.n_tris : 0;
@@ -279,7 +255,91 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.n_nodes = geom.n_nodes;
     kp.n_tris = geom.n_tris;
     kp.n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
-    c->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next);
+    img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next);
+    return XMC_OK;
+}
+
+void fill_ledger(const unsigned long long* L, uint32_t w0_fx, uint64_t n, xmc_ledger* led) {
+    std::memset(led, 0, sizeof(*led));
+    led->photons_launched = L[L_LAUNCHED];
+    led->photons_terminated = L[L_TERMINATED];
+    led->steps = L[L_STEPS];
+    led->n_escaped_top = L[L_N_TOP];
+    led->n_escaped_bottom = L[L_N_BOTTOM];
+    led->n_area = L[L_N_AREA];
+    led->n_cut = L[L_N_CUT];
+    led->n_roulette = L[L_N_ROULETTE];
+    led->n_glass = L[L_N_GLASS];
+    led->n_budget = L[L_N_BUDGET];
+    led->n_invalid = L[L_N_INVALID];
+    led->n_detected = L[L_N_DETECTED];
+    led->n_fp64_retests = L[L_N_RETEST];
+    led->n_node_visits = L[L_N_NODES];
+    led->n_triangle_tests = L[L_N_TRIS];
+    led->specular_fx = (unsigned long long)(kWeightOne - w0_fx) * L[L_LAUNCHED];
+    led->absorbed_fx = L[L_ABSORBED];
+    led->absorbed_outside_fx = L[L_ABSORBED_OUT];
+    led->escaped_top_fx = L[L_TOP];
+    led->escaped_bottom_fx = L[L_BOTTOM];
+    led->lost_area_fx = L[L_AREA];
+    led->lost_cut_fx = L[L_CUT];
+    led->lost_glass_fx = L[L_GLASS];
+    led->lost_budget_fx = L[L_BUDGET];
+    led->lost_invalid_fx = L[L_INVALID];
+    led->roulette_killed_fx = L[L_RKILLED];
+    led->roulette_gained_fx = L[L_RGAINED];
+    const double np = n > 0 ? (double)n : 1.0;
+    const double s = 1.0 / kWeightScale / np;
+    led->specular = (double)led->specular_fx * s;
+    led->absorbed = (double)led->absorbed_fx * s;
+    led->absorbed_outside = (double)led->absorbed_outside_fx * s;
+    led->escaped_top = (double)led->escaped_top_fx * s;
+    led->escaped_bottom = (double)led->escaped_bottom_fx * s;
+    led->lost_area = (double)led->lost_area_fx * s;
+    led->lost_cut = (double)led->lost_cut_fx * s;
+    led->lost_glass = (double)led->lost_glass_fx * s;
+    led->lost_budget = (double)led->lost_budget_fx * s;
+    led->lost_invalid = (double)led->lost_invalid_fx * s;
+    led->roulette_killed = (double)led->roulette_killed_fx * s;
+    led->roulette_gained = (double)led->roulette_gained_fx * s;
+}
+
+static int create(const InputInfo* in, const xmc_options* opt_in, Context** out) {
+    *out = nullptr;
+    HostImage img;
+    int st = prepare_image(in, opt_in, &img);
+    if (st) return st;
+    const xmc_options& opt = img.opt;
+    const GeomImage& geom = img.geom;
+    const std::vector<int8_t>& next = img.next;
+    const std::vector<DevDetector>& dets = img.dets;
+
+    Context* c = new (std::nothrow) Context();
+    if (!c) return fail(XMC_ERR_DEVICE, "out of host memory");
+    c->opt = opt;
+    c->device = opt.device;
+    c->kp = img.kp;
+    c->rsp = img.rsp;
+    c->w0_fx = img.w0_fx;
+    c->grid_size = img.grid_size;
+    c->n_dets = img.n_dets;
+    c->n_time = img.n_time;
+    c->smem_bytes = img.smem_bytes;
+    KParams& kp = c->kp;
+    const int nd = img.n_dets, T = img.n_time;
+    auto bail = [&](int s) { free_context(c); return s; };
+    {
+        cudaError_t e = cudaSetDevice(c->device);
+        if (e != cudaSuccess) return bail(fail(XMC_ERR_DEVICE, std::string("cudaSetDevice: ") + cudaGetErrorString(e)));
+    }
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return bail(fail(XMC_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_))); \
+    } while (0)
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, c->device));
+    c->num_sms = prop.multiProcessorCount;
 
     // ---- device buffers ----
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -401,48 +461,7 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         }
     }
     if (led) {
-        std::memset(led, 0, sizeof(*led));
-        led->photons_launched = L[L_LAUNCHED];
-        led->photons_terminated = L[L_TERMINATED];
-        led->steps = L[L_STEPS];
-        led->n_escaped_top = L[L_N_TOP];
-        led->n_escaped_bottom = L[L_N_BOTTOM];
-        led->n_area = L[L_N_AREA];
-        led->n_cut = L[L_N_CUT];
-        led->n_roulette = L[L_N_ROULETTE];
-        led->n_glass = L[L_N_GLASS];
-        led->n_budget = L[L_N_BUDGET];
-        led->n_invalid = L[L_N_INVALID];
-        led->n_detected = L[L_N_DETECTED];
-        led->n_fp64_retests = L[L_N_RETEST];
-        led->n_node_visits = L[L_N_NODES];
-        led->n_triangle_tests = L[L_N_TRIS];
-        led->specular_fx = (unsigned long long)(kWeightOne - c->w0_fx) * L[L_LAUNCHED];
-        led->absorbed_fx = L[L_ABSORBED];
-        led->absorbed_outside_fx = L[L_ABSORBED_OUT];
-        led->escaped_top_fx = L[L_TOP];
-        led->escaped_bottom_fx = L[L_BOTTOM];
-        led->lost_area_fx = L[L_AREA];
-        led->lost_cut_fx = L[L_CUT];
-        led->lost_glass_fx = L[L_GLASS];
-        led->lost_budget_fx = L[L_BUDGET];
-        led->lost_invalid_fx = L[L_INVALID];
-        led->roulette_killed_fx = L[L_RKILLED];
-        led->roulette_gained_fx = L[L_RGAINED];
-        const double np = n > 0 ? (double)n : 1.0;
-        const double s = inv_scale / np;
-        led->specular = (double)led->specular_fx * s;
-        led->absorbed = (double)led->absorbed_fx * s;
-        led->absorbed_outside = (double)led->absorbed_outside_fx * s;
-        led->escaped_top = (double)led->escaped_top_fx * s;
-        led->escaped_bottom = (double)led->escaped_bottom_fx * s;
-        led->lost_area = (double)led->lost_area_fx * s;
-        led->lost_cut = (double)led->lost_cut_fx * s;
-        led->lost_glass = (double)led->lost_glass_fx * s;
-        led->lost_budget = (double)led->lost_budget_fx * s;
-        led->lost_invalid = (double)led->lost_invalid_fx * s;
-        led->roulette_killed = (double)led->roulette_killed_fx * s;
-        led->roulette_gained = (double)led->roulette_gained_fx * s;
+        fill_ledger(L, c->w0_fx, n, led);
         led->kernel_ms = k_ms;
         led->total_ms = t_ms;
         led->h2d_bytes = c->h2d_bytes + sizeof(KParams);

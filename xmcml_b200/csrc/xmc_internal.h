@@ -137,8 +137,6 @@ struct Context {
     unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;
     unsigned long long* h_tbin = nullptr; unsigned long long* h_ledger = nullptr;
     int* h_status = nullptr;
-    // time bin edges of the reference (FP64), for OutputInfo
-    std::vector<double> bin_start, bin_finish;
     uint64_t last_n = 0;
     double last_kernel_ms = 0.0, last_total_ms = 0.0;
     uint64_t h2d_bytes = 0;   // bytes uploaded by xmc_create (device image)
@@ -150,6 +148,25 @@ struct GeomImage {
     std::vector<float4> tris;    // 3 per triangle
     int n_nodes = 0, n_tris = 0;
 };
+
+// Everything the kernel needs, built on the host from an InputInfo (no device memory yet): kernel
+// parameters with null device pointers, and the arrays they will point to.
+struct HostImage {
+    xmc_options opt{};
+    KParams kp{};
+    GeomImage geom;
+    std::vector<int8_t> next;        // [n_surf * MAX_LAYERS]
+    std::vector<DevDetector> dets;   // [max(1, n_dets)]
+    double rsp = 0.0;
+    uint32_t w0_fx = 0;
+    int grid_size = 0, n_dets = 0, n_time = 0;
+    size_t smem_bytes = 0;
+};
+
+// capi.cpp: validate `in` and build its host image (options normalised as xmc_create does).
+int prepare_image(const InputInfo* in, const xmc_options* opt, HostImage* img);
+// capi.cpp: fill a ledger from the raw device ledger slots of a run of n photons.
+void fill_ledger(const unsigned long long* raw, uint32_t w0_fx, uint64_t n, xmc_ledger* led);
 
 // bvh.cpp
 bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err);

@@ -295,6 +295,28 @@ int xmc_destroy(xmc_context* ctx);
 int xmc_launch(const InputInfo* input, OutputInfo* output, uint64_t seed,
                uint64_t first_photon_id, const xmc_options* opt, xmc_ledger* ledger);
 
+/* No counterpart in the reference. A transport run that allocates no GPU memory, for callers that
+ * cannot call cudaMalloc: code running inside a host framework that owns all device memory through
+ * its own pool, or a process that must not grow its device footprint once it is running. The
+ * caller passes the model (`input`, host memory, as for xmc_create) and its own device buffers for
+ * the raw 64-bit fixed-point outputs (weight 1.0 == 2^31), which the call zeroes and then fills:
+ *   d_absorption [gridSize]; d_detectors [4 * D] (weight, count, target weight, weight^2 per
+ *   detector, D = cube + ring detectors, at least 1); d_time_bins [4 * D * timeScaleSize];
+ *   d_ledger [32] (raw energy-ledger slots).
+ * The device copy of the model (BVH nodes, triangles, layer transitions, detectors) and the
+ * photon-id dispenser live in one static device array of XMC_NOALLOC_SCRATCH_BYTES (8 MiB) that
+ * every GPU loading the library holds until exit; a model that needs more is rejected with
+ * XMC_ERR_RANGE (a mesh of up to roughly 100,000 triangles fits). The first call on a device looks
+ * up that array's device address, so make it once before any stream capture. All calls share the
+ * array and it keeps the last call's contents: calls that overlap on the GPU (on different streams
+ * or threads) race and must be serialised by the caller. `stream` is a cudaStream_t (NULL = the
+ * default stream); the call returns after the run has finished on it. No host event, pinned buffer
+ * or device allocation is made; the only host memory used is ordinary heap for the model image. */
+#define XMC_NOALLOC_SCRATCH_BYTES (8u << 20)
+int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, uint64_t seed, uint64_t first_photon_id,
+                    uint64_t n_photons, unsigned long long* d_absorption, unsigned long long* d_detectors,
+                    unsigned long long* d_time_bins, unsigned long long* d_ledger, void* stream);
+
 /* Replaces LaunchOMP(InputInfo*, OutputInfo*, MCG59*, int)
  * (base/xmcml/xmcmlLauncher/launcher_omp.h:10, launcher_omp.cpp:123-163): runs
  * input->numberOfPhotons photons on the GPU and adds the tallies to `output` (output->

@@ -58,6 +58,8 @@ def load(path: str | None = None) -> C.CDLL:
         "xmc_free_bvh_tree": (None, [P(S.BVHTree)]),
         "xmc_debug_nearest": (C.c_int, [P(S.InputInfo), C.c_int, P(C.c_float), C.c_float, C.c_float,
                                         P(C.c_float), P(C.c_int), P(C.c_float)]),
+        "xmc_run_noalloc": (C.c_int, [P(S.InputInfo), P(S.XmcOptions), C.c_uint64, C.c_uint64, C.c_uint64,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -83,5 +85,5 @@ EXPORTS = [
     "xmc_cancel", "xmc_destroy", "xmc_launch", "xmc_launch_omp", "xmc_init_output", "xmc_free_output",
     "xmc_parse_input_file", "xmc_parse_surface_file", "xmc_free_input", "xmc_write_output_file",
     "xmc_specular_reflectance", "xmc_philox4x32_10", "xmc_layout_offsets", "xmc_device_philox",
-    "xmc_generate_bvh_tree", "xmc_free_bvh_tree", "xmc_debug_nearest",
+    "xmc_generate_bvh_tree", "xmc_free_bvh_tree", "xmc_debug_nearest", "xmc_run_noalloc",
 ]

@@ -200,11 +200,8 @@ def run_e2e(args, m, N, rank, local, world, barrier, dist, torch):
         api.launch_omp(m, out, rng, 0)
         e2e_t.append(time.perf_counter() - t0)
     barrier()
-    e2e_s = sum(e2e_t)
-    if dist is not None:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = tt.item()
+    from xmcml_b200 import replicas
+    e2e_s = replicas.max_over_ranks(sum(e2e_t), dist, torch.device(f"cuda:{local}"))
     e2e_value = world * args.e2e_steps * N / e2e_s
     grid = out.info.gridSize
     D = out.info.numberOfDetectors
@@ -271,9 +268,9 @@ def main():
     t = api.Transport(m, roulette=True, device=local)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
 
-    base = rank * (args.warmup + args.steps) * N  # disjoint photon ids per rank and step
-    for w in range(args.warmup):
-        t.run(N, seed=777, first_photon=base + w * N)
+    from xmcml_b200 import replicas
+    for w in range(args.warmup):  # disjoint photon ids per rank and step
+        t.run(N, seed=777, first_photon=replicas.photon_range(rank, world, N, w)[0])
     barrier()
     leds = []
     with ClockSampler(local) as clk:
@@ -281,15 +278,12 @@ def main():
         for k in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            leds.append(t.run(N, seed=777, first_photon=base + (args.warmup + k) * N))
+            leds.append(t.run(N, seed=777, first_photon=replicas.photon_range(rank, world, N, args.warmup + k)[0]))
         barrier()
     clocks = clk.summary()
-    dev_ms = sum(l["total_ms"] for l in leds)
-    ker_ms = sum(l["kernel_ms"] for l in leds)
-    if dist is not None:
-        tt = torch.tensor([dev_ms, ker_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_ms, ker_ms = tt.tolist()
+    dev = torch.device(f"cuda:{local}")
+    dev_ms = replicas.max_over_ranks(sum(l["total_ms"] for l in leds), dist, dev)
+    ker_ms = replicas.max_over_ranks(sum(l["kernel_ms"] for l in leds), dist, dev)
     value = world * args.steps * N / (dev_ms / 1e3)
     tal = t.tallies()
     last = leds[-1]

@@ -210,7 +210,8 @@ typedef enum xmc_status {
 #define XMC_NO_AREA_KILL    (1u << 1)  /* photons leaving Area keep walking; their absorption goes to
                                           the ledger's absorbed_outside term                         */
 #define XMC_SCATTERING_MAP  (1u << 2)  /* tally the z-plane crossing map OutputInfo.scattering         */
-#define XMC_DETECTOR_TRAJ   (1u << 3)  /* tally per-detector trajectory maps DetectorInfo.trajectory   */
+#define XMC_DETECTOR_TRAJ   (1u << 3)  /* tally per-detector trajectory maps DetectorInfo.trajectory
+                                          (a second, replay pass over the detected photons)         */
 #define XMC_LARGE_GRID      (1u << 4)  /* accept Area partitions above 256 per axis (the reference wraps
                                           voxel indices at 256; this library indexes them in full)    */
 
@@ -242,6 +243,7 @@ typedef struct xmc_ledger {
     uint64_t n_fp64_retests;       /* ray-triangle tests redone in FP64 in an edge band          */
     uint64_t n_node_visits;        /* BVH nodes visited by all ray queries                      */
     uint64_t n_triangle_tests;     /* ray-triangle tests                                        */
+    uint64_t n_replay_mismatch;    /* trajectory replay: photons whose replayed exit differed (0) */
     uint64_t specular_fx, absorbed_fx, absorbed_outside_fx, escaped_top_fx, escaped_bottom_fx,
              lost_area_fx, lost_cut_fx, lost_glass_fx, lost_budget_fx, lost_invalid_fx,
              roulette_killed_fx, roulette_gained_fx;
@@ -286,6 +288,11 @@ int xmc_read_tallies(xmc_context* ctx, uint64_t* absorption, uint64_t* det_weigh
                      uint64_t* time_weight, uint64_t* time_count, uint64_t* time_target,
                      uint64_t* time_weight2);
 
+/* The z-plane crossing tallies of the last xmc_run (host arrays, either may be NULL): the
+ * scattering map [gridSize] in weight fixed point (context created with XMC_SCATTERING_MAP) and the
+ * detector trajectory maps [numberOfDetectors * gridSize] as crossing counts (XMC_DETECTOR_TRAJ). */
+int xmc_read_maps(xmc_context* ctx, uint64_t* scattering, uint64_t* trajectory);
+
 /* Ask a running xmc_run on another thread to stop after the photons in flight. */
 int xmc_cancel(xmc_context* ctx);
 
@@ -321,7 +328,8 @@ int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, uint64_t see
  * (base/xmcml/xmcmlLauncher/launcher_omp.h:10, launcher_omp.cpp:123-163): runs
  * input->numberOfPhotons photons on the GPU and adds the tallies to `output` (output->
  * numberOfPhotons is left to the caller, as the reference does). The counter-RNG key is
- * randomGenerator[0].value and the photons are ids 0..numberOfPhotons-1; afterwards
+ * randomGenerator[0].value and the photons are ids 0..numberOfPhotons-1 (all of LaunchOMP's
+ * tallies are filled, including the scattering map and the detector trajectory maps); afterwards
  * randomGenerator[0] is advanced by one MCG59 step, so consecutive calls (the reference's backup
  * portions, launcher_mpi.cpp:357-380) use fresh keys. numThreads is ignored. Default options
  * (reference semantics: weight cut at minWeight, photons killed outside Area). Returns 0 on

@@ -178,6 +178,45 @@ def test_split_runs_add_up(tmp_path):
     t.close()
 
 
+@pytest.mark.parametrize("which", ["planar", "heightfield"])
+def test_scattering_and_trajectory_maps(tmp_path, which):
+    """UpdatePhotonTrajectory / UpdateDetectorTrajectory (mcml_kernel.cpp:750-810): the scattering map
+    (weight at every z-plane crossing through voxel centres) and, per detector, the crossing counts
+    of the photons it detected (GPU: replay pass over the detected photons)."""
+    n = 50_000
+    sc = scenes.planar(photons=n) if which == "planar" else scenes.height_field_tissue(photons=n, grid=64, time_bins=10)
+    xml, surf = sc.write(str(tmp_path), "maps_" + which)
+    m = api.Model(xml, surf)
+    t = api.Transport(m, roulette=True, scattering=True, trajectories=True)
+    led = t.run(n, seed=31)
+    maps = t.maps()
+    tal = t.tallies()
+    t.close()
+    assert led["n_replay_mismatch"] == 0
+    out = api.Output(m)
+    opts = oracle_opts_for(roulette=True)
+    opts.flags |= B.OFLAG_SCATTERING | B.OFLAG_TRAJECTORY
+    B.oracle_run(m.info, out.info, opts, seed=31, n=n)
+    G = out.info.gridSize
+    osc = np.ctypeslib.as_array(out.info.scattering, shape=(G,))
+    gsc = maps["scattering"].astype(float) / WEIGHT_SCALE
+    shape = m.grid_shape
+    gz, oz = gsc.reshape(shape).sum(axis=(0, 1)), osc.reshape(shape).sum(axis=(0, 1))
+    big = oz > 0.02 * oz.max()
+    print(which, "scattering total", gsc.sum() / n, osc.sum() / n, "max rel slab diff", np.max(np.abs(gz - oz)[big] / oz[big]))
+    assert abs(gsc.sum() - osc.sum()) / osc.sum() < 5e-3
+    assert np.max(np.abs(gz - oz)[big] / oz[big]) < 0.03
+    D = m.n_detectors
+    otr = np.stack([np.ctypeslib.as_array(out.info.detectorInfo[d].trajectory, shape=(G,)) for d in range(D)])
+    gtr = maps["trajectory"][:D]
+    gt, ot = gtr.sum(axis=1).astype(float), otr.sum(axis=1).astype(float)
+    sel = ot > 1000
+    print(which, "trajectory totals (first 5)", gt[:5], ot[:5])
+    assert np.all(np.abs(gt - ot)[sel] / ot[sel] < 0.03)
+    # every detected photon was replayed: detector counts of the run pass equal those of the oracle
+    assert np.array_equal(tal["det_count"][:D] > 0, out.detector_counts() > 0)
+
+
 def test_launch_omp_shim_accumulates(tmp_path):
     n = 20_000
     xml, surf = scenes.planar(photons=n).write(str(tmp_path), "omp")
@@ -194,6 +233,10 @@ def test_launch_omp_shim_accumulates(tmp_path):
     w2 = out.detector_weights().sum()
     assert 1.8 * w1 < w2 < 2.2 * w1
     assert out.detector_counts().sum() > 0 and out.absorption.sum() > 0
+    # LaunchOMP fills the scattering map and the detector trajectory maps too
+    assert np.ctypeslib.as_array(out.info.scattering, shape=(out.info.gridSize,)).sum() > 0
+    assert sum(np.ctypeslib.as_array(out.info.detectorInfo[d].trajectory, shape=(out.info.gridSize,)).sum()
+               for d in range(out.info.numberOfDetectors)) > 0
     p = str(tmp_path / "r.mcml.out")
     out.write(p)
     assert os.path.getsize(p) > out.info.gridSize * 8

@@ -40,6 +40,7 @@ def load(path: str | None = None) -> C.CDLL:
         "xmc_run": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, P(S.OutputInfo), P(S.XmcLedger)]),
         "xmc_read_tallies": (C.c_int, [C.c_void_p] + [P(C.c_uint64)] * 9),
         "xmc_cancel": (C.c_int, [C.c_void_p]),
+        "xmc_read_maps": (C.c_int, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
         "xmc_destroy": (C.c_int, [C.c_void_p]),
         "xmc_launch": (C.c_int, [P(S.InputInfo), P(S.OutputInfo), C.c_uint64, C.c_uint64, P(S.XmcOptions),
                                  P(S.XmcLedger)]),
@@ -82,7 +83,7 @@ def check(status: int) -> int:
 # Exported C-ABI symbols, as declared in include/xmcml_b200.h.
 EXPORTS = [
     "xmc_version", "xmc_last_error", "xmc_default_options", "xmc_create", "xmc_run", "xmc_read_tallies",
-    "xmc_cancel", "xmc_destroy", "xmc_launch", "xmc_launch_omp", "xmc_init_output", "xmc_free_output",
+    "xmc_cancel", "xmc_read_maps", "xmc_destroy", "xmc_launch", "xmc_launch_omp", "xmc_init_output", "xmc_free_output",
     "xmc_parse_input_file", "xmc_parse_surface_file", "xmc_free_input", "xmc_write_output_file",
     "xmc_specular_reflectance", "xmc_philox4x32_10", "xmc_layout_offsets", "xmc_device_philox",
     "xmc_generate_bvh_tree", "xmc_free_bvh_tree", "xmc_debug_nearest", "xmc_run_noalloc",

@@ -101,11 +101,13 @@ class Output:
 
 def options(roulette: bool = False, area_kill: bool = True, beam_radius: float = 0.0, chance: float = 0.1,
             device: int = 0, block_size: int = 0, blocks_per_sm: int = 0, photons_per_chunk: int = 0,
-            smem_nodes: int = 0, max_steps: int = 0, large_grid: bool = False) -> S.XmcOptions:
+            smem_nodes: int = 0, max_steps: int = 0, large_grid: bool = False, scattering: bool = False,
+            trajectories: bool = False) -> S.XmcOptions:
     o = S.XmcOptions()
     load().xmc_default_options(C.byref(o))
     o.flags = (S.XMC_ROULETTE if roulette else 0) | (0 if area_kill else S.XMC_NO_AREA_KILL) | \
-              (S.XMC_LARGE_GRID if large_grid else 0)
+              (S.XMC_LARGE_GRID if large_grid else 0) | (S.XMC_SCATTERING_MAP if scattering else 0) | \
+              (S.XMC_DETECTOR_TRAJ if trajectories else 0)
     o.roulette_chance = chance
     o.beam_radius = beam_radius
     o.device = device
@@ -152,6 +154,20 @@ class Transport:
         for k in ("time_weight", "time_count", "time_target", "time_weight2"):
             arr[k] = arr[k].reshape(D, T)
         return arr
+
+    def maps(self) -> dict:
+        """Scattering map [grid] (weight fixed point) and trajectory maps [detectors, grid] (counts)."""
+        res = {}
+        P = C.POINTER(C.c_uint64)
+        if self.opts.flags & S.XMC_SCATTERING_MAP:
+            a = np.zeros(self.grid, dtype=np.uint64)
+            check(self._lib.xmc_read_maps(self._ctx, a.ctypes.data_as(P), None))
+            res["scattering"] = a
+        if self.opts.flags & S.XMC_DETECTOR_TRAJ:
+            a = np.zeros(max(self.n_dets, 1) * self.grid, dtype=np.uint64)
+            check(self._lib.xmc_read_maps(self._ctx, None, a.ctypes.data_as(P)))
+            res["trajectory"] = a.reshape(max(self.n_dets, 1), self.grid)
+        return res
 
     def cancel(self):
         self._lib.xmc_cancel(self._ctx)

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "xmc_internal.h"
 
@@ -33,7 +34,8 @@ static void free_context(Context* c) {
     int dev = -1;
     if (cudaGetDevice(&dev) == cudaSuccess && dev != c->device) cudaSetDevice(c->device);
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
-                     c->d_tbin, c->d_ledger, c->d_counter, c->d_status};
+                     c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
+                     c->d_replay, c->d_replay_count, c->d_replay_ledger};
     for (void* p : dbufs)
         if (p) cudaFree(p);
     void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status};
@@ -96,8 +98,6 @@ static int validate(const InputInfo* in, const xmc_options& opt) {
     if ((long long)in->timeScaleSize * (in->numberOfCubeDetectors + in->numberOfRingDetectors) > (1ll << 26))
         return fail(XMC_ERR_RANGE, "time-bin tally too large");
     if (in->useBiasing) return fail(XMC_ERR_UNSUPPORTED, "biasing (attractive point) is not provided by the GPU path");
-    if (opt.flags & (XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ))
-        return fail(XMC_ERR_UNSUPPORTED, "scattering map and detector trajectory tallies are not provided by the GPU path");
     for (int l = 0; l < in->numberOfLayers; ++l) {
         const LayerInfo& L = in->layerInfo[l];
         if (L.numberOfSurfaces < 0 || (L.numberOfSurfaces > 0 && !L.surfaceId))
@@ -180,6 +180,9 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.byte_sentinel = (A.partitionNumber.x >= 256 && A.partitionNumber.y >= 256 && A.partitionNumber.z >= 256 &&
                         !(opt.flags & XMC_LARGE_GRID)) ? 1 : 0;
     img->grid_size = A.partitionNumber.x * A.partitionNumber.y * A.partitionNumber.z;
+    kp.grid = img->grid_size;
+    kp.plane_dz = (float)(A.length.z / A.partitionNumber.z);
+    kp.area_zend = (float)(A.corner.z + A.length.z);
     // ---- detectors: cubes then rings (GetDetectorId order, mcml_kernel.cpp:663-742) ----
     const int nd = in->numberOfCubeDetectors + in->numberOfRingDetectors;
     std::vector<DevDetector>& dets = img->dets;
@@ -365,6 +368,12 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     CK(cudaMalloc(&c->d_ledger, led_b));
     CK(cudaMalloc(&c->d_counter, 16));
     CK(cudaMalloc(&c->d_status, 16));
+    if (opt.flags & XMC_SCATTERING_MAP) CK(cudaMalloc(&c->d_scatter, absorb_b));
+    if (opt.flags & XMC_DETECTOR_TRAJ) {
+        CK(cudaMalloc(&c->d_traj, absorb_b * (size_t)std::max(1, nd)));
+        CK(cudaMalloc(&c->d_replay_count, 16));
+        CK(cudaMalloc(&c->d_replay_ledger, led_b));
+    }
     CK(cudaHostAlloc((void**)&c->h_cancel, 16, cudaHostAllocMapped));
     *c->h_cancel = 0;
     CK(cudaHostAlloc((void**)&c->h_absorb, absorb_b, cudaHostAllocDefault));
@@ -385,6 +394,9 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.counter = (unsigned long long*)c->d_counter;
     kp.cancel = d_cancel;
     kp.status = (int*)c->d_status;
+    kp.scatter = (unsigned long long*)c->d_scatter;
+    kp.traj = (unsigned long long*)c->d_traj;
+    kp.replay_count = (unsigned long long*)c->d_replay_count;
 
     // ---- launch shape ----
     c->block = opt.block_size > 0 ? opt.block_size : 256;
@@ -419,8 +431,55 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     XMC_CUDA(cudaMemsetAsync(c->d_ledger, 0, led_b, c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_counter, 0, 16, c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_status, 0, 16, c->stream));
+    const bool traj = (c->opt.flags & XMC_DETECTOR_TRAJ) != 0;
+    const bool scat = (c->opt.flags & XMC_SCATTERING_MAP) != 0;
+    if (scat) XMC_CUDA(cudaMemsetAsync(c->d_scatter, 0, absorb_b, c->stream));
+    if (traj) {
+        XMC_CUDA(cudaMemsetAsync(c->d_traj, 0, absorb_b * (size_t)std::max(1, c->n_dets), c->stream));
+        XMC_CUDA(cudaMemsetAsync(c->d_replay_ledger, 0, led_b, c->stream));
+    }
     XMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
-    if (n > 0) XMC_CUDA(enqueue_transport(c));
+    if (n > 0 && !traj) XMC_CUDA(enqueue_transport(c));
+    if (n > 0 && traj) {
+        // Detector trajectory maps in two passes per portion of photons: the run pass lists every
+        // detected photon as (index, detector); the replay pass walks exactly those photons again
+        // (same counter-RNG draws, same code) and counts their z-plane crossings in that
+        // detector's map. The reference keeps a per-photon crossing log instead
+        // (PhotonTrajectory, mcml_kernel_types.h:118-124).
+        const uint64_t portion_max = 1ull << 26;
+        const uint64_t cap = std::min<uint64_t>(n, portion_max);
+        if (c->replay_cap < cap) {
+            if (c->d_replay) cudaFree(c->d_replay);
+            c->d_replay = nullptr;
+            c->replay_cap = 0;
+            XMC_CUDA(cudaMalloc(&c->d_replay, sizeof(unsigned long long) * cap));
+            c->replay_cap = cap;
+        }
+        for (uint64_t done = 0; done < n; done += portion_max) {
+            const uint64_t portion = std::min(portion_max, n - done);
+            kp.mode = 0;
+            kp.first_id = first + done;
+            kp.n_photons = portion;
+            kp.replay_list = (unsigned long long*)c->d_replay;
+            kp.replay_cap = c->replay_cap;
+            kp.ledger = (unsigned long long*)c->d_ledger;
+            XMC_CUDA(cudaMemsetAsync(c->d_counter, 0, 16, c->stream));
+            XMC_CUDA(cudaMemsetAsync(c->d_replay_count, 0, 16, c->stream));
+            XMC_CUDA(enqueue_transport(c));
+            unsigned long long listed = 0;
+            XMC_CUDA(cudaMemcpyAsync(&listed, c->d_replay_count, sizeof(listed), cudaMemcpyDeviceToHost, c->stream));
+            XMC_CUDA(cudaStreamSynchronize(c->stream));
+            kp.mode = 1;
+            kp.n_photons = std::min<unsigned long long>(listed, c->replay_cap);
+            kp.ledger = (unsigned long long*)c->d_replay_ledger;
+            XMC_CUDA(cudaMemsetAsync(c->d_counter, 0, 16, c->stream));
+            if (kp.n_photons) XMC_CUDA(enqueue_transport(c));
+            kp.mode = 0;
+            kp.ledger = (unsigned long long*)c->d_ledger;
+        }
+        kp.first_id = first;
+        kp.n_photons = n;
+    }
     XMC_CUDA(cudaEventRecord(c->ev[2], c->stream));
     if (out) XMC_CUDA(cudaMemcpyAsync(c->h_absorb, c->d_absorb, absorb_b, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaMemcpyAsync(c->h_det, c->d_det, det_b, cudaMemcpyDeviceToHost, c->stream));
@@ -467,6 +526,28 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         led->h2d_bytes = c->h2d_bytes + sizeof(KParams);
         led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16;
     }
+    if (out && scat && out->scattering) {
+        std::vector<unsigned long long> m((size_t)c->grid_size);
+        XMC_CUDA(cudaMemcpy(m.data(), c->d_scatter, absorb_b, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < c->grid_size; ++i) out->scattering[i] += (double)m[i] * inv_scale;
+    }
+    unsigned long long mismatch = 0;
+    if (traj) {
+        unsigned long long rl[kLedgerSlots];
+        XMC_CUDA(cudaMemcpy(rl, c->d_replay_ledger, led_b, cudaMemcpyDeviceToHost));
+        mismatch = rl[L_N_REPLAY_MISMATCH];
+        if (out) {
+            std::vector<unsigned long long> m((size_t)c->grid_size);
+            for (int d = 0; d < c->n_dets; ++d) {
+                DetectorInfo& D = out->detectorInfo[d];
+                if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
+                XMC_CUDA(cudaMemcpy(m.data(), (unsigned long long*)c->d_traj + (size_t)d * c->grid_size, absorb_b,
+                                    cudaMemcpyDeviceToHost));
+                for (int i = 0; i < c->grid_size; ++i) D.trajectory[i] += m[i];
+            }
+        }
+    }
+    if (led) led->n_replay_mismatch = mismatch;
     if (c->h_status[0] & 2) return fail(XMC_ERR_CANCELLED, "run cancelled");
     if (c->h_status[0] & 1) return fail(XMC_ERR_BUDGET, "a photon reached the step budget and was terminated");
     return XMC_OK;
@@ -538,6 +619,22 @@ int xmc_read_tallies(xmc_context* ctx, uint64_t* absorption, uint64_t* det_weigh
     return XMC_OK;
 }
 
+int xmc_read_maps(xmc_context* ctx, uint64_t* scattering, uint64_t* trajectory) {
+    if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
+    Context* c = reinterpret_cast<Context*>(ctx);
+    XMC_CUDA(cudaSetDevice(c->device));
+    const size_t b = sizeof(unsigned long long) * (size_t)c->grid_size;
+    if (scattering) {
+        if (!c->d_scatter) return fail(XMC_ERR_INVALID_INPUT, "context was created without XMC_SCATTERING_MAP");
+        XMC_CUDA(cudaMemcpy(scattering, c->d_scatter, b, cudaMemcpyDeviceToHost));
+    }
+    if (trajectory) {
+        if (!c->d_traj) return fail(XMC_ERR_INVALID_INPUT, "context was created without XMC_DETECTOR_TRAJ");
+        XMC_CUDA(cudaMemcpy(trajectory, c->d_traj, b * (size_t)std::max(1, c->n_dets), cudaMemcpyDeviceToHost));
+    }
+    return XMC_OK;
+}
+
 int xmc_cancel(xmc_context* ctx) {
     if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
     Context* c = reinterpret_cast<Context*>(ctx);
@@ -569,7 +666,10 @@ int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* rng, int numThre
         std::fprintf(stderr, "xmc_launch_omp: %s\n", xmc_last_error());
         return XMC_ERR_INVALID_INPUT;
     }
-    int st = xmc_launch(input, output, rng[0].value, 0, nullptr, nullptr);
+    xmc_options opt;
+    xmc_default_options(&opt);
+    opt.flags = XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ;  // every tally LaunchOMP fills
+    int st = xmc_launch(input, output, rng[0].value, 0, &opt, nullptr);
     if (st && st != XMC_ERR_BUDGET) {
         std::fprintf(stderr, "xmc_launch_omp: %s\n", xmc_last_error());
         return st;

@@ -66,6 +66,10 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     HostImage img;
     int st = prepare_image(input, opt, &img);
     if (st) return st;
+    if (img.opt.flags & (XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ)) {
+        set_error("xmc_run_noalloc: scattering and trajectory maps need buffers this entry point does not take");
+        return XMC_ERR_UNSUPPORTED;
+    }
     const GeomImage& geom = img.geom;
 
     // scratch layout: [dispenser u64 | status int] [nodes] [triangles] [transition table] [detectors]

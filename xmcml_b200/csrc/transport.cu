@@ -51,6 +51,7 @@ struct Photon {
     int excl;
     float tmin;
     float gap_lo, gap_hi;  // triangle-free z-gap containing the photon (empty if none)
+    int rdet;              // replay pass: the detector this photon reached in the run pass
     unsigned long long pid;
 };
 
@@ -96,8 +97,7 @@ __device__ __forceinline__ void lat(unsigned long long* p, unsigned long long v)
 
 // mcml_kernel.cpp:663-742 (first matching cube, then ring; layer filter; angle test) and the
 // detector tallies of :744-858. Weight arithmetic in fixed point.
-__device__ void detect_and_tally(const KParams& P, const SmemTally& S, const DevDetector* __restrict__ s_det,
-                                 const Photon& ph) {
+__device__ int find_detector(const KParams& P, const DevDetector* __restrict__ s_det, const Photon& ph) {
     int det = -1;
     const float l2 = ph.dx * ph.dx + ph.dy * ph.dy + ph.dz * ph.dz;
     const float ac = -ph.dz / l2;
@@ -117,7 +117,10 @@ __device__ void detect_and_tally(const KParams& P, const SmemTally& S, const Dev
             break;
         }
     }
-    if (det < 0) return;
+    return det;
+}
+
+__device__ void tally_detection(const KParams& P, const SmemTally& S, const Photon& ph, int det) {
     const uint32_t w = ph.w;
     const float total = ph.trange + ph.orange;
     const uint32_t tw = total > 0.0f ? __float2uint_rn(__uint2float_rn(w) * (ph.trange / total)) : 0u;
@@ -139,6 +142,36 @@ __device__ void detect_and_tally(const KParams& P, const SmemTally& S, const Dev
         atomicAdd(tb + 1, 1ull);
         lat(tb + 2, tw);
         lat(tb + 3, w2);
+    }
+}
+
+// UpdatePhotonTrajectory (mcml_kernel.cpp:750-792): for a move from p0 to p1, every z-plane through
+// voxel centres between them (inside Area) is crossed at one voxel. The run pass adds the photon's
+// weight to the scattering map there; the replay pass counts the crossing in the trajectory map of
+// the detector the photon reaches (UpdateDetectorTrajectory, :794-810), which the reference does by
+// replaying a per-photon crossing log at detection.
+__device__ void cross_planes(const KParams& P, float x0, float y0, float z0, float x1, float y1, float z1, uint32_t w,
+                             int rdet) {
+    if (z1 == z0) return;
+    float sx = x0, sy = y0, sz = z0, fz = z1, ex = x1 - x0, ey = y1 - y0, ez = z1 - z0;
+    if (z1 < z0) {
+        sx = x1; sy = y1; sz = z1; fz = z0;
+        ex = -ex; ey = -ey; ez = -ez;
+    }
+    const float step = P.plane_dz;
+    const int k = (int)((sz - P.az + 0.5f * step) / step);
+    float plane = P.az + k * step + 0.5f * step;
+    const float inv = 1.0f / ez;
+    for (int guard = 0; plane <= fz && plane < P.area_zend && guard < 65536; ++guard) {
+        const float t = (plane - sz) * inv;
+        const int idx = area_index(P, fmaf(ex, t, sx), fmaf(ey, t, sy), plane, 0.0f);
+        if (idx < 0) break;
+        if (P.mode == 0) {
+            if (w) atomicAdd(&P.scatter[idx], (unsigned long long)w);
+        } else {
+            atomicAdd(&P.traj[(size_t)rdet * P.grid + idx], 1ull);
+        }
+        plane += step;
     }
 }
 
@@ -209,6 +242,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     const unsigned lt_mask = (1u << lane) - 1u;
     const bool area_kill = !(P.flags & XMC_NO_AREA_KILL);
     const bool roulette = (P.flags & XMC_ROULETTE) != 0;
+    const bool record_planes = P.mode == 1 || (P.flags & XMC_SCATTERING_MAP) != 0;
 
     unsigned long long cbeg = 0, cend = 0;  // warp-uniform chunk of photon indices
     bool exhausted = false;                 // warp-uniform
@@ -244,7 +278,14 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             const int cnt = __popc(need);
             const int take = (int)min((unsigned long long)cnt, avail);
             if (((need >> lane) & 1u) && rank < take) {
-                launch_photon(P, ph, P.first_id + cbeg + rank);
+                unsigned long long idx = cbeg + rank;
+                ph.rdet = -1;
+                if (P.mode == 1) {
+                    const unsigned long long e = P.replay_list[idx];
+                    idx = e >> 16;
+                    ph.rdet = (int)(e & 0xffffu);
+                }
+                launch_photon(P, ph, P.first_id + idx);
                 find_gap(s_zlo, s_zhi, P.n_zocc, ph.pz, ph.gap_lo, ph.gap_hi);
                 alive = true;
                 atomicAdd(&S.ledger[L_LAUNCHED], 1ull);
@@ -294,9 +335,11 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             u_roulette = boundary ? u24(r.z) : u24(r.w);
         }
         // move (mcml_kernel.cpp:151-174): optical path length, target/other range
+        const float ox = ph.px, oy = ph.py, oz = ph.pz;
         ph.px = fmaf(step, ph.dx, ph.px);
         ph.py = fmaf(step, ph.dy, ph.py);
         ph.pz = fmaf(step, ph.dz, ph.pz);
+        if (record_planes) cross_planes(P, ox, oy, oz, ph.px, ph.py, ph.pz, ph.w, ph.rdet);
         ph.time = fmaf(step, L.n, ph.time);
         if (!(ph.pz > ph.gap_lo && ph.pz < ph.gap_hi)) find_gap(s_zlo, s_zhi, P.n_zocc, ph.pz, ph.gap_lo, ph.gap_hi);
         if ((P.target_mask >> ph.layer) & 1u) ph.trange += step;
@@ -371,7 +414,19 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             if (u_fresnel > R) {
                 if (next == 0) {
                     // leaves the tissue: detectors (mcml_kernel.cpp:257-268)
-                    detect_and_tally(P, S, s_det, ph);
+                    const int det = find_detector(P, s_det, ph);
+                    if (P.mode == 0) {
+                        if (det >= 0) {
+                            tally_detection(P, S, ph, det);
+                            if (P.flags & XMC_DETECTOR_TRAJ) {
+                                const unsigned long long slot = atomicAdd(P.replay_count, 1ull);
+                                if (slot < P.replay_cap)
+                                    P.replay_list[slot] = ((ph.pid - P.first_id) << 16) | (unsigned long long)det;
+                            }
+                        }
+                    } else if (det != ph.rdet) {
+                        atomicAdd(&S.ledger[L_N_REPLAY_MISMATCH], 1ull);
+                    }
                     if (ph.dz < 0.0f) kill(S, ph, alive, L_N_TOP, L_TOP);
                     else kill(S, ph, alive, L_N_BOTTOM, L_BOTTOM);
                     continue;
@@ -401,7 +456,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             dw = min(dw, ph.w);
             ph.w -= dw;
             if (idx >= 0) {
-                if (dw) atomicAdd(&P.absorb[idx], (unsigned long long)dw);
+                if (dw && P.mode == 0) atomicAdd(&P.absorb[idx], (unsigned long long)dw);
                 absorbed += dw;
             } else {
                 absorbed_out += dw;

@@ -63,7 +63,7 @@ enum LedgerSlot {
     L_N_TOP, L_N_BOTTOM, L_N_AREA, L_N_CUT, L_N_ROULETTE, L_N_GLASS, L_N_BUDGET, L_N_INVALID,
     L_N_DETECTED, L_N_RETEST, L_N_NODES, L_N_TRIS,
     L_ABSORBED, L_ABSORBED_OUT, L_TOP, L_BOTTOM, L_AREA, L_CUT, L_GLASS, L_BUDGET, L_INVALID,
-    L_RKILLED, L_RGAINED,
+    L_RKILLED, L_RGAINED, L_N_REPLAY_MISMATCH,
     L_COUNT
 };
 constexpr int kLedgerSlots = 32;  // padded
@@ -106,6 +106,16 @@ struct KParams {
     uint32_t key0, key1;      // Philox key (seed)
     unsigned long long first_id, n_photons, max_steps;
     int chunk;
+    // z-plane crossing tallies (UpdatePhotonTrajectory): planes at voxel centres
+    float plane_dz;           // Area length.z / partitions.z
+    float area_zend;          // corner.z + length.z
+    int grid;                 // nx * ny * nz
+    int mode;                 // 0: transport run, 1: trajectory replay of detected photons
+    unsigned long long* scatter;        // [grid] scattering map (XMC_SCATTERING_MAP), weight fixed point
+    unsigned long long* traj;           // [n_dets * grid] detector trajectory maps (replay pass), counts
+    unsigned long long* replay_list;    // run: (index << 16 | detector) of detected photons; replay: input
+    unsigned long long* replay_count;   // run: number of entries written
+    unsigned long long replay_cap;      // run: capacity of replay_list
     // tallies (device, fixed point)
     unsigned long long* absorb;   // [nx*ny*nz]
     unsigned long long* det;      // [n_dets * 4]: weight, count, target weight, weight^2
@@ -132,6 +142,9 @@ struct Context {
     void* d_nodes = nullptr; void* d_tris = nullptr; void* d_next = nullptr; void* d_dets = nullptr;
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
     void* d_counter = nullptr; void* d_status = nullptr;
+    void* d_scatter = nullptr; void* d_traj = nullptr; void* d_replay = nullptr; void* d_replay_count = nullptr;
+    void* d_replay_ledger = nullptr;
+    unsigned long long replay_cap = 0;
     int* h_cancel = nullptr;  // pinned, mapped
     // pinned read-back buffers
     unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;

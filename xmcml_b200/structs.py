@@ -128,7 +128,7 @@ class XmcOptions(C.Structure):
 
 _LEDGER_COUNTS = ["photons_launched", "photons_terminated", "steps", "n_escaped_top", "n_escaped_bottom",
                   "n_area", "n_cut", "n_roulette", "n_glass", "n_budget", "n_invalid", "n_detected",
-                  "n_fp64_retests", "n_node_visits", "n_triangle_tests"]
+                  "n_fp64_retests", "n_node_visits", "n_triangle_tests", "n_replay_mismatch"]
 LEDGER_TERMS = ["specular", "absorbed", "absorbed_outside", "escaped_top", "escaped_bottom", "lost_area",
                 "lost_cut", "lost_glass", "lost_budget", "lost_invalid", "roulette_killed", "roulette_gained"]
 

@@ -310,10 +310,10 @@ int xmc_launch(const InputInfo* input, OutputInfo* output, uint64_t seed,
  *   d_absorption [gridSize]; d_detectors [4 * D] (weight, count, target weight, weight^2 per
  *   detector, D = cube + ring detectors, at least 1); d_time_bins [4 * D * timeScaleSize];
  *   d_ledger [32] (raw energy-ledger slots).
- * The device copy of the model (BVH nodes, triangles, layer transitions, detectors) and the
- * photon-id dispenser live in one static device array of XMC_NOALLOC_SCRATCH_BYTES (8 MiB) that
- * every GPU loading the library holds until exit; a model that needs more is rejected with
- * XMC_ERR_RANGE (a mesh of up to roughly 100,000 triangles fits). The first call on a device looks
+ * The device copy of the model (BVH nodes, triangles, layer transitions, detectors, xy cell grid)
+ * and the photon-id dispenser live in one static device array of XMC_NOALLOC_SCRATCH_BYTES (8 MiB)
+ * that every GPU loading the library holds until exit; a model that needs more is rejected with
+ * XMC_ERR_RANGE (a mesh of up to roughly 50,000 triangles fits). The first call on a device looks
  * up that array's device address, so make it once before any stream capture. All calls share the
  * array and it keeps the last call's contents: calls that overlap on the GPU (on different streams
  * or threads) race and must be serialised by the caller. `stream` is a cudaStream_t (NULL = the
@@ -371,9 +371,10 @@ int xmc_layout_offsets(int64_t* out, int max_count);
 
 /* Self test of the kernel's ray query compiled for the host: for each ray (ox,oy,oz,dx,dy,dz in
  * rays[6*i]) the nearest hit with tmin <= t <= tmax over the device image of `input` (distance,
- * surface id or -1, unit normal or NULL). Used by the CPU test suite. */
+ * surface id or -1, unit normal or NULL), through the xy cell grid where the kernel would use it
+ * (use_grid != 0) or the BVH only. Used by the CPU test suite. */
 int xmc_debug_nearest(const InputInfo* input, int n_rays, const float* rays, float tmin, float tmax,
-                      float* t_out, int* surf_out, float* normal_out);
+                      float* t_out, int* surf_out, float* normal_out, int use_grid);
 
 /* Run the photon kernel's device-side self test: `n` Philox blocks for the given key written to
  * out[4*n] (device path), for comparing with xmc_philox4x32_10. */

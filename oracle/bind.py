@@ -100,6 +100,8 @@ def oracle() -> C.CDLL:
         lib.oracle_kat_refract.argtypes = [D, D, pd, pd, pd]
         lib.oracle_detector_id.restype = C.c_int
         lib.oracle_detector_id.argtypes = [P(S.InputInfo), S.double3, S.double3, P(C.c_bool)]
+        lib.oracle_kat_nearest_batch.restype = C.c_int
+        lib.oracle_kat_nearest_batch.argtypes = [P(S.InputInfo), C.c_int, pd, D, C.c_int, pd, P(C.c_int), pd]
         lib.oracle_kat_nearest.restype = C.c_int
         lib.oracle_kat_nearest.argtypes = [P(S.InputInfo), pd, pd, D, C.c_int, pd, P(C.c_int), pd]
         _oracle = lib

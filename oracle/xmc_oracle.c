@@ -953,3 +953,22 @@ int oracle_kat_nearest(const InputInfo* in, const double* o, const double* d, do
     if (h.isFindIntersection) { normal[0] = h.normal.x; normal[1] = h.normal.y; normal[2] = h.normal.z; }
     return h.isFindIntersection;
 }
+
+/* The same for n rays (rays[6*i]: origin, direction) over one geometry build. */
+int oracle_kat_nearest_batch(const InputInfo* in, int n, const double* rays, double step, int bounded,
+                             double* dist, int* surf, double* normal) {
+    o_geom* g = o_geom_create(in);
+    int hits = 0;
+    for (int i = 0; i < n; ++i) {
+        const double* q = rays + 6 * (size_t)i;
+        IntersectionInfo h = o_nearest(g, v3(q[0], q[1], q[2]), v3(q[3], q[4], q[5]), step, bounded);
+        dist[i] = h.distance;
+        surf[i] = h.isFindIntersection ? h.surfaceId : -1;
+        if (h.isFindIntersection) {
+            normal[3 * (size_t)i] = h.normal.x; normal[3 * (size_t)i + 1] = h.normal.y; normal[3 * (size_t)i + 2] = h.normal.z;
+            ++hits;
+        }
+    }
+    o_geom_free(g);
+    return hits;
+}

@@ -58,7 +58,7 @@ def load(path: str | None = None) -> C.CDLL:
         "xmc_generate_bvh_tree": (P(S.BVHTree), [P(S.Surface), C.c_int]),
         "xmc_free_bvh_tree": (None, [P(S.BVHTree)]),
         "xmc_debug_nearest": (C.c_int, [P(S.InputInfo), C.c_int, P(C.c_float), C.c_float, C.c_float,
-                                        P(C.c_float), P(C.c_int), P(C.c_float)]),
+                                        P(C.c_float), P(C.c_int), P(C.c_float), C.c_int]),
         "xmc_run_noalloc": (C.c_int, [P(S.InputInfo), P(S.XmcOptions), C.c_uint64, C.c_uint64, C.c_uint64,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     }

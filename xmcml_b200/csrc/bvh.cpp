@@ -357,6 +357,88 @@ int occupied_z_slabs(const GeomImage& g, float* lo, float* hi) {
     return (int)m.size();
 }
 
+void build_xy_grid(const GeomImage& g, GridImage* out) {
+    *out = GridImage();
+    if (g.n_tris == 0) return;
+    float xlo = INFINITY, ylo = INFINITY, xhi = -INFINITY, yhi = -INFINITY;
+    for (int i = 0; i < g.n_tris; ++i)
+        for (int c = 0; c < 3; ++c) {
+            const float4 v = g.tris[3 * (size_t)i + c];
+            xlo = std::min(xlo, v.x); xhi = std::max(xhi, v.x);
+            ylo = std::min(ylo, v.y); yhi = std::max(yhi, v.y);
+        }
+    const float padx = 1e-5f * std::max(1.0f, std::max(std::fabs(xlo), std::fabs(xhi)));
+    const float pady = 1e-5f * std::max(1.0f, std::max(std::fabs(ylo), std::fabs(yhi)));
+    xlo -= padx; xhi += padx; ylo -= pady; yhi += pady;
+    const double wx = std::max(1e-6f, xhi - xlo), wy = std::max(1e-6f, yhi - ylo);
+    // about two triangles per cell, square-ish cells, at most 1024 x 1024
+    const double cells = std::min(1048576.0, std::max(1.0, g.n_tris / 2.0));
+    int nx = (int)std::ceil(std::sqrt(cells * wx / wy));
+    nx = std::max(1, std::min(1024, nx));
+    int ny = (int)std::ceil(cells / nx);
+    ny = std::max(1, std::min(1024, ny));
+    out->nx = nx;
+    out->ny = ny;
+    out->x0 = xlo;
+    out->y0 = ylo;
+    out->icx = (float)(nx / wx);
+    out->icy = (float)(ny / wy);
+    const size_t nc = (size_t)nx * ny;
+    struct Span { int i0, i1, j0, j1; float zl, zh; };
+    std::vector<Span> spans(g.n_tris);
+    for (int t = 0; t < g.n_tris; ++t) {
+        float ax = INFINITY, bx = -INFINITY, ay = INFINITY, by = -INFINITY, zl = INFINITY, zh = -INFINITY;
+        for (int c = 0; c < 3; ++c) {
+            const float4 v = g.tris[3 * (size_t)t + c];
+            ax = std::min(ax, v.x); bx = std::max(bx, v.x);
+            ay = std::min(ay, v.y); by = std::max(by, v.y);
+            zl = std::min(zl, v.z); zh = std::max(zh, v.z);
+        }
+        const float pz = 1e-5f * std::max(1.0f, std::max(std::fabs(zl), std::fabs(zh)));
+        Span& sp = spans[t];
+        sp.zl = zl - pz;
+        sp.zh = zh + pz;
+        sp.i0 = std::max(0, std::min(nx - 1, (int)std::floor((ax - padx - xlo) * out->icx)));
+        sp.i1 = std::max(0, std::min(nx - 1, (int)std::floor((bx + padx - xlo) * out->icx)));
+        sp.j0 = std::max(0, std::min(ny - 1, (int)std::floor((ay - pady - ylo) * out->icy)));
+        sp.j1 = std::max(0, std::min(ny - 1, (int)std::floor((by + pady - ylo) * out->icy)));
+    }
+    auto as_float = [](int t) { float f; std::memcpy(&f, &t, sizeof(f)); return f; };
+    std::vector<char> is_big(g.n_tris, 0);
+    for (int t = 0; t < g.n_tris && (int)(out->big.size() / 4) < kMaxBigTriangles; ++t) {
+        const Span& sp = spans[t];
+        const long long covered = (long long)(sp.i1 - sp.i0 + 1) * (sp.j1 - sp.j0 + 1);
+        if (covered > kBigTriangleCells) {
+            is_big[t] = 1;
+            out->big.push_back(make_float4(sp.zl, sp.zh, as_float(t), 0.0f));
+            for (int c = 0; c < 3; ++c) out->big.push_back(g.tris[3 * (size_t)t + c]);
+        }
+    }
+    std::vector<unsigned int> count(nc, 0);
+    for (int t = 0; t < g.n_tris; ++t) {
+        if (is_big[t]) continue;
+        const Span& sp = spans[t];
+        for (int j = sp.j0; j <= sp.j1; ++j)
+            for (int i = sp.i0; i <= sp.i1; ++i) count[(size_t)j * nx + i]++;
+    }
+    out->cells.resize(nc);
+    unsigned int acc = 0;
+    for (size_t c = 0; c < nc; ++c) {
+        out->cells[c] = make_uint2(acc, count[c]);
+        acc += count[c];
+    }
+    out->entries.resize(acc);
+    std::vector<unsigned int> fill(nc);
+    for (size_t c = 0; c < nc; ++c) fill[c] = out->cells[c].x;
+    for (int t = 0; t < g.n_tris; ++t) {
+        if (is_big[t]) continue;
+        const Span& sp = spans[t];
+        for (int j = sp.j0; j <= sp.j1; ++j)
+            for (int i = sp.i0; i <= sp.i1; ++i)
+                out->entries[fill[(size_t)j * nx + i]++] = make_float4(sp.zl, sp.zh, as_float(t), 0.0f);
+    }
+}
+
 // GenerateBVHTree replacement (mcml_intersection.cpp:316-344): a binned-SAH tree of this library
 // returned in the reference's own BVHTree layout (FP64 boxes, leaves as (surfId, trIndex) runs,
 // nodes listed children-before-parent with the root last, as the reference emits them), so callers

@@ -35,7 +35,8 @@ static void free_context(Context* c) {
     if (cudaGetDevice(&dev) == cudaSuccess && dev != c->device) cudaSetDevice(c->device);
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
                      c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
-                     c->d_replay, c->d_replay_count, c->d_replay_ledger};
+                     c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_entries,
+                     c->d_big, c->d_cancel};
     for (void* p : dbufs)
         if (p) cudaFree(p);
     void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status};
@@ -44,6 +45,7 @@ static void free_context(Context* c) {
     for (cudaEvent_t& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->cancel_stream) cudaStreamDestroy(c->cancel_stream);
     delete c;
 }
 
@@ -208,6 +210,14 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     }
     kp.n_cubes = in->numberOfCubeDetectors;
     kp.n_rings = in->numberOfRingDetectors;
+    kp.rings_sorted = in->numberOfRingDetectors > 1 ? 1 : 0;
+    for (int i = 0; i < in->numberOfRingDetectors && kp.rings_sorted; ++i) {
+        const RingDetector& R = in->ringDetector[i];
+        if (R.center.x != in->ringDetector[0].center.x || R.center.y != in->ringDetector[0].center.y ||
+            !(R.smallRadius <= R.bigRadius))
+            kp.rings_sorted = 0;
+        if (i > 0 && !(in->ringDetector[i - 1].bigRadius <= R.smallRadius)) kp.rings_sorted = 0;
+    }
     kp.n_dets = nd;
     img->n_dets = nd;
     // ---- time bins: InitOutput (launcher_omp.cpp:36-55) ----
@@ -258,6 +268,14 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.n_nodes = geom.n_nodes;
     kp.n_tris = geom.n_tris;
     kp.n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
+    build_xy_grid(geom, &img->grid);
+    kp.grid_x0 = img->grid.x0;
+    kp.grid_y0 = img->grid.y0;
+    kp.grid_icx = img->grid.icx;
+    kp.grid_icy = img->grid.icy;
+    kp.grid_nx = img->grid.nx;
+    kp.grid_ny = img->grid.ny;
+    kp.n_big = (int)(img->grid.big.size() / 4);
     img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next);
     return XMC_OK;
 }
@@ -358,6 +376,10 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     CK(up(&c->d_tris, geom.tris.data(), sizeof(float4) * geom.tris.size()));
     CK(up(&c->d_next, next.data(), next.size()));
     CK(up(&c->d_dets, dets.data(), sizeof(DevDetector) * dets.size()));
+    CK(up(&c->d_cells, img.grid.cells.data(), sizeof(uint2) * img.grid.cells.size()));
+    CK(up(&c->d_cell_entries, img.grid.entries.data(), sizeof(float4) * img.grid.entries.size()));
+    CK(up(&c->d_big, img.grid.big.data(), sizeof(float4) * img.grid.big.size()));
+    c->h2d_bytes += sizeof(uint2) * img.grid.cells.size() + sizeof(float4) * (img.grid.entries.size() + img.grid.big.size());
     const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
     const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, nd);
     const size_t tbin_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, nd) * T;
@@ -374,25 +396,28 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
         CK(cudaMalloc(&c->d_replay_count, 16));
         CK(cudaMalloc(&c->d_replay_ledger, led_b));
     }
-    CK(cudaHostAlloc((void**)&c->h_cancel, 16, cudaHostAllocMapped));
-    *c->h_cancel = 0;
+    CK(cudaHostAlloc((void**)&c->h_cancel, 16, cudaHostAllocDefault));
+    *c->h_cancel = 1;
+    CK(cudaMalloc(&c->d_cancel, 16));
+    CK(cudaStreamCreateWithFlags(&c->cancel_stream, cudaStreamNonBlocking));
     CK(cudaHostAlloc((void**)&c->h_absorb, absorb_b, cudaHostAllocDefault));
     CK(cudaHostAlloc((void**)&c->h_det, det_b, cudaHostAllocDefault));
     CK(cudaHostAlloc((void**)&c->h_tbin, tbin_b, cudaHostAllocDefault));
     CK(cudaHostAlloc((void**)&c->h_ledger, led_b, cudaHostAllocDefault));
     CK(cudaHostAlloc((void**)&c->h_status, 16, cudaHostAllocDefault));
-    int* d_cancel = nullptr;
-    CK(cudaHostGetDevicePointer((void**)&d_cancel, c->h_cancel, 0));
     kp.nodes = (const float4*)c->d_nodes;
     kp.tris = (const float4*)c->d_tris;
     kp.next_layer = (const int8_t*)c->d_next;
     kp.dets = (const DevDetector*)c->d_dets;
+    kp.cells = (const uint2*)c->d_cells;
+    kp.cell_entries = (const float4*)c->d_cell_entries;
+    kp.big = (const float4*)c->d_big;
     kp.absorb = (unsigned long long*)c->d_absorb;
     kp.det = (unsigned long long*)c->d_det;
     kp.tbin = (unsigned long long*)c->d_tbin;
     kp.ledger = (unsigned long long*)c->d_ledger;
     kp.counter = (unsigned long long*)c->d_counter;
-    kp.cancel = d_cancel;
+    kp.cancel = (const volatile int*)c->d_cancel;
     kp.status = (int*)c->d_status;
     kp.scatter = (unsigned long long*)c->d_scatter;
     kp.traj = (unsigned long long*)c->d_traj;
@@ -419,7 +444,6 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     kp.key1 = (uint32_t)(seed >> 32);
     kp.first_id = first;
     kp.n_photons = n;
-    *c->h_cancel = 0;
     const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
     const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, c->n_dets);
     const size_t tbin_b = det_b * c->n_time;
@@ -431,6 +455,7 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     XMC_CUDA(cudaMemsetAsync(c->d_ledger, 0, led_b, c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_counter, 0, 16, c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_status, 0, 16, c->stream));
+    XMC_CUDA(cudaMemsetAsync(c->d_cancel, 0, 16, c->stream));
     const bool traj = (c->opt.flags & XMC_DETECTOR_TRAJ) != 0;
     const bool scat = (c->opt.flags & XMC_SCATTERING_MAP) != 0;
     if (scat) XMC_CUDA(cudaMemsetAsync(c->d_scatter, 0, absorb_b, c->stream));
@@ -638,7 +663,10 @@ int xmc_read_maps(xmc_context* ctx, uint64_t* scattering, uint64_t* trajectory) 
 int xmc_cancel(xmc_context* ctx) {
     if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
     Context* c = reinterpret_cast<Context*>(ctx);
-    *(volatile int*)c->h_cancel = 1;
+    // the running kernel polls d_cancel; write it from a second stream so the copy does not queue
+    // behind the kernel on the run stream
+    XMC_CUDA(cudaMemcpyAsync(c->d_cancel, c->h_cancel, sizeof(int), cudaMemcpyHostToDevice, c->cancel_stream));
+    XMC_CUDA(cudaStreamSynchronize(c->cancel_stream));
     return XMC_OK;
 }
 

@@ -135,4 +135,75 @@ __host__ __device__ __forceinline__ Hit bvh_nearest(const float4* __restrict__ g
     return h;
 }
 
+// One ray-triangle candidate of the grid search: nearest wins, equal distances keep the lower index.
+__host__ __device__ __forceinline__ void grid_candidate(float4 a, float4 b, float4 c, int t, float ox, float oy, float oz,
+                                                        float dx, float dy, float dz, float tmin, unsigned& retests,
+                                                        Hit& h) {
+    const float d = tri_distance(a, b, c, ox, oy, oz, dx, dy, dz, retests);
+    if (d >= tmin && d < INFINITY && (d < h.t || (d == h.t && (h.tri < 0 || t < h.tri)))) {
+        h.t = d;
+        h.tri = t;
+    }
+}
+
+// Nearest hit with tmin <= t <= tmax for a bounded segment: the big triangles (shared memory) and
+// the cells under the segment's xy bounding box, entries culled by z-range, loaded four at a time so
+// their fetches overlap. Returns false when the box covers more than kGridMaxCells cells; the caller
+// then uses the BVH.
+__host__ __device__ __forceinline__ bool grid_nearest(const uint2* __restrict__ cells, const float4* __restrict__ entries,
+                                                      const float4* __restrict__ big, int n_big, float gx0, float gy0,
+                                                      float icx, float icy, int nx, int ny,
+                                                      const float4* __restrict__ g_tris, const float4* __restrict__ s_tris,
+                                                      int n_smem_tris, float ox, float oy, float oz, float dx, float dy,
+                                                      float dz, float tmin, float tmax, int excl, unsigned& retests,
+                                                      unsigned& n_visit, unsigned& n_tri, Hit& h) {
+    const float ex = fmaf(dx, tmax, ox), ey = fmaf(dy, tmax, oy), ez = fmaf(dz, tmax, oz);
+    const float fx0 = fminf(fmaxf((fminf(ox, ex) - gx0) * icx, -1.0f), (float)nx);
+    const float fx1 = fminf(fmaxf((fmaxf(ox, ex) - gx0) * icx, -1.0f), (float)nx);
+    const float fy0 = fminf(fmaxf((fminf(oy, ey) - gy0) * icy, -1.0f), (float)ny);
+    const float fy1 = fminf(fmaxf((fmaxf(oy, ey) - gy0) * icy, -1.0f), (float)ny);
+    h.t = tmax;
+    h.tri = -1;
+    if (!(fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)nx && fy0 < (float)ny)) return true;  // outside every triangle
+    const int i0 = max(0, (int)floorf(fx0)), i1 = min(nx - 1, (int)floorf(fx1));
+    const int j0 = max(0, (int)floorf(fy0)), j1 = min(ny - 1, (int)floorf(fy1));
+    if ((i1 - i0 + 1) * (j1 - j0 + 1) > kGridMaxCells) return false;
+    const float zl = fminf(oz, ez), zh = fmaxf(oz, ez);
+    for (int k = 0; k < n_big; ++k) {
+        const float4 en = big[4 * k];
+        if (en.y < zl || en.x > zh) continue;
+        const int t = f2i(en.z);
+        if (t == excl) continue;
+        ++n_tri;
+        grid_candidate(big[4 * k + 1], big[4 * k + 2], big[4 * k + 3], t, ox, oy, oz, dx, dy, dz, tmin, retests, h);
+    }
+    for (int j = j0; j <= j1; ++j) {
+        for (int i = i0; i <= i1; ++i) {
+            const uint2 cell = XMC_LDG(&cells[(unsigned int)j * (unsigned int)nx + (unsigned int)i]);
+            n_visit += 1;
+            for (unsigned int k = 0; k < cell.y; k += 4) {
+                float4 en[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    en[q] = k + q < cell.y ? XMC_LDG(&entries[cell.x + k + q]) : make_float4(INFINITY, -INFINITY, 0.0f, 0.0f);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (en[q].y < zl || en[q].x > zh) continue;
+                    const int t = f2i(en[q].z);
+                    if (t == excl) continue;
+                    float4 a, b, c;
+                    if (t < n_smem_tris) {
+                        a = s_tris[3 * t]; b = s_tris[3 * t + 1]; c = s_tris[3 * t + 2];
+                    } else {
+                        a = XMC_LDG(&g_tris[3 * t]); b = XMC_LDG(&g_tris[3 * t + 1]); c = XMC_LDG(&g_tris[3 * t + 2]);
+                    }
+                    ++n_tri;
+                    grid_candidate(a, b, c, t, ox, oy, oz, dx, dy, dz, tmin, retests, h);
+                }
+            }
+        }
+    }
+    return true;
+}
+
 }  // namespace xmc

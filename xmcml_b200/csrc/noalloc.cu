@@ -5,8 +5,8 @@
 // start-up (allocation there fails, stalls on a device-wide synchronisation, or fragments the
 // pool). Such a caller brings the output buffers from its own memory. Everything else the kernel
 // needs beyond its inputs and outputs (the device copy of the tissue model: BVH nodes, triangle
-// records, layer-transition table and detector records, plus the photon-id dispenser and the
-// status word) is scratch, and it lives here in one file-scope __device__ array of fixed size,
+// records, layer-transition table, detector records and the xy cell grid, plus the photon-id
+// dispenser and the status word) is scratch, and it lives here in one file-scope __device__ array of fixed size,
 // which every GPU that loads the library holds until the process exits.
 #include <cstring>
 #include <mutex>
@@ -72,16 +72,23 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     }
     const GeomImage& geom = img.geom;
 
-    // scratch layout: [dispenser u64 | status int] [nodes] [triangles] [transition table] [detectors]
+    // scratch layout: [dispenser u64 | status int | cancel int] [nodes] [triangles] [transition table]
+    // [detectors] [grid cells] [grid entries] [big triangles]
     const size_t b_nodes = sizeof(float4) * geom.nodes.size();
     const size_t b_tris = sizeof(float4) * geom.tris.size();
     const size_t b_next = img.next.size();
     const size_t b_dets = sizeof(DevDetector) * img.dets.size();
+    const size_t b_cells = sizeof(uint2) * img.grid.cells.size();
+    const size_t b_entries = sizeof(float4) * img.grid.entries.size();
+    const size_t b_big = sizeof(float4) * img.grid.big.size();
     const size_t o_nodes = kAlign;
     const size_t o_tris = o_nodes + align_up(b_nodes);
     const size_t o_next = o_tris + align_up(b_tris);
     const size_t o_dets = o_next + align_up(b_next);
-    const size_t need = o_dets + align_up(b_dets);
+    const size_t o_cells = o_dets + align_up(b_dets);
+    const size_t o_entries = o_cells + align_up(b_cells);
+    const size_t o_big = o_entries + align_up(b_entries);
+    const size_t need = o_big + align_up(b_big);
     if (need > kNoAllocScratchBytes) {
         set_error("xmc_run_noalloc: the model needs " + std::to_string(need) + " bytes of device scratch; this entry "
                   "point holds at most " + std::to_string(kNoAllocScratchBytes) + " (use xmc_create/xmc_run)");
@@ -109,6 +116,9 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     kp.tris = reinterpret_cast<const float4*>(scratch + o_tris);
     kp.next_layer = reinterpret_cast<const int8_t*>(scratch + o_next);
     kp.dets = reinterpret_cast<const DevDetector*>(scratch + o_dets);
+    kp.cells = reinterpret_cast<const uint2*>(scratch + o_cells);
+    kp.cell_entries = reinterpret_cast<const float4*>(scratch + o_entries);
+    kp.big = reinterpret_cast<const float4*>(scratch + o_big);
     kp.counter = reinterpret_cast<unsigned long long*>(scratch);
     kp.status = reinterpret_cast<int*>(scratch + sizeof(unsigned long long));
     kp.cancel = nullptr;
@@ -151,6 +161,10 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     if (b_tris) NA_CK(cudaMemcpyAsync(scratch + o_tris, geom.tris.data(), b_tris, cudaMemcpyHostToDevice, c.stream));
     NA_CK(cudaMemcpyAsync(scratch + o_next, img.next.data(), b_next, cudaMemcpyHostToDevice, c.stream));
     NA_CK(cudaMemcpyAsync(scratch + o_dets, img.dets.data(), b_dets, cudaMemcpyHostToDevice, c.stream));
+    if (b_cells) NA_CK(cudaMemcpyAsync(scratch + o_cells, img.grid.cells.data(), b_cells, cudaMemcpyHostToDevice, c.stream));
+    if (b_entries)
+        NA_CK(cudaMemcpyAsync(scratch + o_entries, img.grid.entries.data(), b_entries, cudaMemcpyHostToDevice, c.stream));
+    if (b_big) NA_CK(cudaMemcpyAsync(scratch + o_big, img.grid.big.data(), b_big, cudaMemcpyHostToDevice, c.stream));
     const size_t nd = (size_t)std::max(1, img.n_dets);
     NA_CK(cudaMemsetAsync(d_absorption, 0, sizeof(unsigned long long) * (size_t)img.grid_size, c.stream));
     NA_CK(cudaMemsetAsync(d_detectors, 0, sizeof(unsigned long long) * 4 * nd, c.stream));

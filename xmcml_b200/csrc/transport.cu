@@ -101,7 +101,8 @@ __device__ int find_detector(const KParams& P, const DevDetector* __restrict__ s
     int det = -1;
     const float l2 = ph.dx * ph.dx + ph.dy * ph.dy + ph.dz * ph.dz;
     const float ac = -ph.dz / l2;
-    for (int i = 0; i < P.n_dets; ++i) {
+    const int n_scan = P.rings_sorted ? P.n_cubes : P.n_dets;
+    for (int i = 0; i < n_scan; ++i) {
         const DevDetector D = s_det[i];
         bool inside;
         if (i < P.n_cubes) {
@@ -116,6 +117,21 @@ __device__ int find_detector(const KParams& P, const DevDetector* __restrict__ s
             det = i;
             break;
         }
+    }
+    if (det < 0 && P.rings_sorted) {
+        // concentric, sorted, non-overlapping rings: the only ring that can contain the radius is
+        // the last one whose small radius is <= r, so the first match of the scan is this one
+        const DevDetector* R = s_det + P.n_cubes;
+        const float ex = ph.px - R[0].cx, ey = ph.py - R[0].cy;
+        const float r = sqrtf(ex * ex + ey * ey);
+        int lo = 0, hi = P.n_rings - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (R[mid].hx <= r) lo = mid;
+            else hi = mid - 1;
+        }
+        const DevDetector D = R[lo];
+        if (r >= D.hx && r < D.hy && (D.filter & ph.visited) && ac > D.cos_angle) det = P.n_cubes + lo;
     }
     return det;
 }
@@ -224,6 +240,8 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     DevDetector* s_det = reinterpret_cast<DevDetector*>(s_layer + MAX_LAYERS);
     int8_t* s_next = reinterpret_cast<int8_t*>(s_det + P.n_dets);
     __shared__ float s_zlo[kMaxZSlabs], s_zhi[kMaxZSlabs];
+    __shared__ float4 s_big[4 * kMaxBigTriangles];
+    for (int i = threadIdx.x; i < 4 * P.n_big; i += blockDim.x) s_big[i] = P.big[i];
     for (int i = threadIdx.x; i < P.n_zocc; i += blockDim.x) {
         s_zlo[i] = P.zocc_lo[i];
         s_zhi[i] = P.zocc_hi[i];
@@ -260,7 +278,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                 unsigned long long b = 0;
                 int cancelled = 0;
                 if (lane == 0) {
-                    if (P.cancel && *P.cancel) cancelled = 1;
+                    if (P.cancel && *P.cancel) cancelled = 1;  // device memory, written by xmc_cancel
                     b = cancelled ? P.n_photons : atomicAdd(P.counter, (unsigned long long)P.chunk);
                 }
                 b = __shfl_sync(FULL, b, 0);
@@ -326,7 +344,10 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             if (fminf(ph.pz, zend) > ph.gap_lo && fmaxf(ph.pz, zend) < ph.gap_hi) {
                 hit.tri = -1;  // the step stays inside a triangle-free z-gap: no surface to cross
                 hit.t = step;
-            } else {
+            } else if (!(P.grid_nx > 0 &&
+                         grid_nearest(P.cells, P.cell_entries, s_big, P.n_big, P.grid_x0, P.grid_y0, P.grid_icx,
+                                      P.grid_icy, P.grid_nx, P.grid_ny, P.tris, s_tris, P.smem_tris, ph.px, ph.py, ph.pz, ph.dx,
+                                      ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri, hit))) {
                 hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
                                   ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
             }
@@ -564,15 +585,22 @@ cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n
 
 // Host run of the kernel's ray query on the geometry image of `in` (self-test of the traversal).
 extern "C" int xmc_debug_nearest(const InputInfo* in, int n_rays, const float* rays, float tmin, float tmax,
-                                 float* t_out, int* surf_out, float* normal_out) {
+                                 float* t_out, int* surf_out, float* normal_out, int use_grid) {
     xmc::GeomImage g;
     std::string err;
     if (!xmc::build_geometry(in, &g, &err)) { xmc::set_error(err); return XMC_ERR_INVALID_INPUT; }
+    xmc::GridImage grid;
+    if (use_grid) xmc::build_xy_grid(g, &grid);
     for (int r = 0; r < n_rays; ++r) {
         const float* q = rays + 6 * (size_t)r;
         unsigned retests = 0, nv = 0, nt = 0;
-        xmc::Hit h = xmc::bvh_nearest(g.nodes.data(), g.tris.data(), g.n_nodes, nullptr, 0, nullptr, 0, q[0], q[1], q[2],
-                                      q[3], q[4], q[5], tmin, tmax, -1, retests, nv, nt);
+        xmc::Hit h;
+        if (!(use_grid && grid.nx > 0 && tmax < INFINITY &&
+              xmc::grid_nearest(grid.cells.data(), grid.entries.data(), grid.big.data(), (int)(grid.big.size() / 4), grid.x0,
+                                grid.y0, grid.icx, grid.icy, grid.nx, grid.ny, g.tris.data(), nullptr, 0, q[0], q[1], q[2],
+                                q[3], q[4], q[5], tmin, tmax, -1, retests, nv, nt, h)))
+            h = xmc::bvh_nearest(g.nodes.data(), g.tris.data(), g.n_nodes, nullptr, 0, nullptr, 0, q[0], q[1], q[2],
+                                 q[3], q[4], q[5], tmin, tmax, -1, retests, nv, nt);
         t_out[r] = h.tri >= 0 ? h.t : INFINITY;
         surf_out[r] = h.tri >= 0 ? xmc::f2i(g.tris[3 * (size_t)h.tri].w) : -1;
         if (normal_out && h.tri >= 0) {

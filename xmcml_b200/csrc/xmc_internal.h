@@ -68,6 +68,15 @@ enum LedgerSlot {
 };
 constexpr int kLedgerSlots = 32;  // padded
 
+// xy cell grid over all triangles for short (bounded) ray queries: each cell lists the triangles
+// whose xy bounding box overlaps it, with their z-range; a query whose xy footprint covers at most
+// kGridMaxCells cells tests those lists, longer ones use the BVH.
+constexpr int kGridMaxCells = 4;
+// Triangles whose xy bounding box covers more than kBigTriangleCells cells (large planes) are kept
+// out of the cells in a short list staged in shared memory (at most kMaxBigTriangles of them).
+constexpr int kBigTriangleCells = 64;
+constexpr int kMaxBigTriangles = 64;
+
 // z-intervals occupied by triangles (merged, padded, sorted): a step whose z-range lies strictly
 // inside a gap between them cannot cross any surface, so its ray query is skipped.
 constexpr int kMaxZSlabs = 24;
@@ -82,6 +91,13 @@ struct KParams {
     int smem_nodes, smem_tris, smem_next;  // how many of each are staged in shared memory
     float zocc_lo[kMaxZSlabs], zocc_hi[kMaxZSlabs];
     int n_zocc;
+    // xy cell grid (grid_nx == 0: none)
+    const uint2* cells;               // [grid_nx * grid_ny]: {first entry, entry count}
+    const float4* cell_entries;       // {zmin, zmax, triangle index (bits), 0}
+    const float4* big;                // [n_big * 4]: {zmin, zmax, triangle index (bits), 0}, then the 3 triangle float4s
+    int n_big;
+    float grid_x0, grid_y0, grid_icx, grid_icy;  // origin and 1 / cell size
+    int grid_nx, grid_ny;
     // layers
     DevLayer layer[MAX_LAYERS];
     int n_layers;
@@ -94,6 +110,8 @@ struct KParams {
     // detectors and time bins
     const DevDetector* dets;
     int n_cubes, n_rings, n_dets;
+    int rings_sorted;         // rings share one centre, are sorted and do not overlap: at most one
+                              // ring contains a radius, found by binary search
     float t0, dt;             // time bins: [t0 + i dt, t0 + (i+1) dt), last bin open-ended
     int n_time;
     // launch
@@ -122,7 +140,7 @@ struct KParams {
     unsigned long long* tbin;     // [n_dets * n_time * 4]
     unsigned long long* ledger;   // [kLedgerSlots]
     unsigned long long* counter;  // photon id dispenser
-    const volatile int* cancel;   // host-mapped cancel flag (may be null)
+    const volatile int* cancel;   // device cancel flag, written by xmc_cancel from another stream (may be null)
     int* status;                  // device status word: bit0 budget hit, bit1 cancelled
 };
 
@@ -142,10 +160,12 @@ struct Context {
     void* d_nodes = nullptr; void* d_tris = nullptr; void* d_next = nullptr; void* d_dets = nullptr;
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
     void* d_counter = nullptr; void* d_status = nullptr;
+    void* d_cells = nullptr; void* d_cell_entries = nullptr; void* d_big = nullptr; void* d_cancel = nullptr;
+    cudaStream_t cancel_stream = nullptr;
     void* d_scatter = nullptr; void* d_traj = nullptr; void* d_replay = nullptr; void* d_replay_count = nullptr;
     void* d_replay_ledger = nullptr;
     unsigned long long replay_cap = 0;
-    int* h_cancel = nullptr;  // pinned, mapped
+    int* h_cancel = nullptr;  // pinned source of the value xmc_cancel writes into d_cancel
     // pinned read-back buffers
     unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;
     unsigned long long* h_tbin = nullptr; unsigned long long* h_ledger = nullptr;
@@ -162,6 +182,15 @@ struct GeomImage {
     int n_nodes = 0, n_tris = 0;
 };
 
+// Host image of the xy cell grid.
+struct GridImage {
+    float x0 = 0, y0 = 0, icx = 0, icy = 0;
+    int nx = 0, ny = 0;
+    std::vector<uint2> cells;
+    std::vector<float4> entries;
+    std::vector<float4> big;      // 4 float4 per big triangle
+};
+
 // Everything the kernel needs, built on the host from an InputInfo (no device memory yet): kernel
 // parameters with null device pointers, and the arrays they will point to.
 struct HostImage {
@@ -170,6 +199,7 @@ struct HostImage {
     GeomImage geom;
     std::vector<int8_t> next;        // [n_surf * MAX_LAYERS]
     std::vector<DevDetector> dets;   // [max(1, n_dets)]
+    GridImage grid;
     double rsp = 0.0;
     uint32_t w0_fx = 0;
     int grid_size = 0, n_dets = 0, n_time = 0;
@@ -185,6 +215,9 @@ void fill_ledger(const unsigned long long* raw, uint32_t w0_fx, uint64_t n, xmc_
 bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err);
 // bvh.cpp: merged z-intervals occupied by the triangles of `g` (at most kMaxZSlabs, conservative)
 int occupied_z_slabs(const GeomImage& g, float* lo, float* hi);
+
+// bvh.cpp: build the xy cell grid over the triangles of `g` (empty grid when there are none)
+void build_xy_grid(const GeomImage& g, GridImage* out);
 
 // transport.cu: enqueue one transport kernel launch on ctx->stream (tallies must be zeroed).
 cudaError_t enqueue_transport(Context* ctx);

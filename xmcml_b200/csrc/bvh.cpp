@@ -437,6 +437,35 @@ void build_xy_grid(const GeomImage& g, GridImage* out) {
             for (int i = sp.i0; i <= sp.i1; ++i)
                 out->entries[fill[(size_t)j * nx + i]++] = make_float4(sp.zl, sp.zh, as_float(t), 0.0f);
     }
+    // per cell: the z-intervals its triangles occupy, merged and reduced to at most 4 (a step whose
+    // z-range misses them all cannot hit a triangle of the cell)
+    out->cell_z.assign(2 * nc, make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY));
+    std::vector<std::pair<float, float>> iv;
+    for (size_t c = 0; c < nc; ++c) {
+        iv.clear();
+        for (unsigned int k = 0; k < out->cells[c].y; ++k) {
+            const float4 e = out->entries[out->cells[c].x + k];
+            iv.push_back({e.x, e.y});
+        }
+        std::sort(iv.begin(), iv.end());
+        std::vector<std::pair<float, float>> m;
+        for (auto& v : iv) {
+            if (!m.empty() && v.first <= m.back().second) m.back().second = std::max(m.back().second, v.second);
+            else m.push_back(v);
+        }
+        while (m.size() > 4) {
+            size_t best = 0;
+            float gap = INFINITY;
+            for (size_t q = 0; q + 1 < m.size(); ++q)
+                if (m[q + 1].first - m[q].second < gap) { gap = m[q + 1].first - m[q].second; best = q; }
+            m[best].second = std::max(m[best].second, m[best + 1].second);
+            m.erase(m.begin() + best + 1);
+        }
+        float z[8] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
+        for (size_t q = 0; q < m.size(); ++q) { z[2 * q] = m[q].first; z[2 * q + 1] = m[q].second; }
+        out->cell_z[2 * c] = make_float4(z[0], z[1], z[2], z[3]);
+        out->cell_z[2 * c + 1] = make_float4(z[4], z[5], z[6], z[7]);
+    }
 }
 
 // GenerateBVHTree replacement (mcml_intersection.cpp:316-344): a binned-SAH tree of this library

@@ -35,7 +35,7 @@ static void free_context(Context* c) {
     if (cudaGetDevice(&dev) == cudaSuccess && dev != c->device) cudaSetDevice(c->device);
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
                      c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
-                     c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_entries,
+                     c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_z, c->d_cell_entries,
                      c->d_big, c->d_cancel};
     for (void* p : dbufs)
         if (p) cudaFree(p);
@@ -377,9 +377,11 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     CK(up(&c->d_next, next.data(), next.size()));
     CK(up(&c->d_dets, dets.data(), sizeof(DevDetector) * dets.size()));
     CK(up(&c->d_cells, img.grid.cells.data(), sizeof(uint2) * img.grid.cells.size()));
+    CK(up(&c->d_cell_z, img.grid.cell_z.data(), sizeof(float4) * img.grid.cell_z.size()));
     CK(up(&c->d_cell_entries, img.grid.entries.data(), sizeof(float4) * img.grid.entries.size()));
     CK(up(&c->d_big, img.grid.big.data(), sizeof(float4) * img.grid.big.size()));
-    c->h2d_bytes += sizeof(uint2) * img.grid.cells.size() + sizeof(float4) * (img.grid.entries.size() + img.grid.big.size());
+    c->h2d_bytes += sizeof(uint2) * img.grid.cells.size() +
+                    sizeof(float4) * (img.grid.cell_z.size() + img.grid.entries.size() + img.grid.big.size());
     const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
     const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, nd);
     const size_t tbin_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, nd) * T;
@@ -410,6 +412,7 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.next_layer = (const int8_t*)c->d_next;
     kp.dets = (const DevDetector*)c->d_dets;
     kp.cells = (const uint2*)c->d_cells;
+    kp.cell_z = (const float4*)c->d_cell_z;
     kp.cell_entries = (const float4*)c->d_cell_entries;
     kp.big = (const float4*)c->d_big;
     kp.absorb = (unsigned long long*)c->d_absorb;

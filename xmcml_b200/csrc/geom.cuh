@@ -150,7 +150,8 @@ __host__ __device__ __forceinline__ void grid_candidate(float4 a, float4 b, floa
 // the cells under the segment's xy bounding box, entries culled by z-range, loaded four at a time so
 // their fetches overlap. Returns false when the box covers more than kGridMaxCells cells; the caller
 // then uses the BVH.
-__host__ __device__ __forceinline__ bool grid_nearest(const uint2* __restrict__ cells, const float4* __restrict__ entries,
+__host__ __device__ __forceinline__ bool grid_nearest(const uint2* __restrict__ cells, const float4* __restrict__ cell_z,
+                                                      const float4* __restrict__ entries,
                                                       const float4* __restrict__ big, int n_big, float gx0, float gy0,
                                                       float icx, float icy, int nx, int ny,
                                                       const float4* __restrict__ g_tris, const float4* __restrict__ s_tris,
@@ -179,8 +180,13 @@ __host__ __device__ __forceinline__ bool grid_nearest(const uint2* __restrict__ 
     }
     for (int j = j0; j <= j1; ++j) {
         for (int i = i0; i <= i1; ++i) {
-            const uint2 cell = XMC_LDG(&cells[(unsigned int)j * (unsigned int)nx + (unsigned int)i]);
+            const unsigned int ci = (unsigned int)j * (unsigned int)nx + (unsigned int)i;
+            const uint2 cell = XMC_LDG(&cells[ci]);
+            const float4 za = XMC_LDG(&cell_z[2 * ci]), zb = XMC_LDG(&cell_z[2 * ci + 1]);
             n_visit += 1;
+            // the cell's occupied z-intervals: skip it when the step's z-range misses all of them
+            if ((za.y < zl || za.x > zh) && (za.w < zl || za.z > zh) && (zb.y < zl || zb.x > zh) && (zb.w < zl || zb.z > zh))
+                continue;
             for (unsigned int k = 0; k < cell.y; k += 4) {
                 float4 en[4];
 #pragma unroll

@@ -73,12 +73,13 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     const GeomImage& geom = img.geom;
 
     // scratch layout: [dispenser u64 | status int | cancel int] [nodes] [triangles] [transition table]
-    // [detectors] [grid cells] [grid entries] [big triangles]
+    // [detectors] [grid cells] [cell z-intervals] [grid entries] [big triangles]
     const size_t b_nodes = sizeof(float4) * geom.nodes.size();
     const size_t b_tris = sizeof(float4) * geom.tris.size();
     const size_t b_next = img.next.size();
     const size_t b_dets = sizeof(DevDetector) * img.dets.size();
     const size_t b_cells = sizeof(uint2) * img.grid.cells.size();
+    const size_t b_cell_z = sizeof(float4) * img.grid.cell_z.size();
     const size_t b_entries = sizeof(float4) * img.grid.entries.size();
     const size_t b_big = sizeof(float4) * img.grid.big.size();
     const size_t o_nodes = kAlign;
@@ -86,7 +87,8 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     const size_t o_next = o_tris + align_up(b_tris);
     const size_t o_dets = o_next + align_up(b_next);
     const size_t o_cells = o_dets + align_up(b_dets);
-    const size_t o_entries = o_cells + align_up(b_cells);
+    const size_t o_cell_z = o_cells + align_up(b_cells);
+    const size_t o_entries = o_cell_z + align_up(b_cell_z);
     const size_t o_big = o_entries + align_up(b_entries);
     const size_t need = o_big + align_up(b_big);
     if (need > kNoAllocScratchBytes) {
@@ -117,6 +119,7 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     kp.next_layer = reinterpret_cast<const int8_t*>(scratch + o_next);
     kp.dets = reinterpret_cast<const DevDetector*>(scratch + o_dets);
     kp.cells = reinterpret_cast<const uint2*>(scratch + o_cells);
+    kp.cell_z = reinterpret_cast<const float4*>(scratch + o_cell_z);
     kp.cell_entries = reinterpret_cast<const float4*>(scratch + o_entries);
     kp.big = reinterpret_cast<const float4*>(scratch + o_big);
     kp.counter = reinterpret_cast<unsigned long long*>(scratch);
@@ -162,6 +165,7 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     NA_CK(cudaMemcpyAsync(scratch + o_next, img.next.data(), b_next, cudaMemcpyHostToDevice, c.stream));
     NA_CK(cudaMemcpyAsync(scratch + o_dets, img.dets.data(), b_dets, cudaMemcpyHostToDevice, c.stream));
     if (b_cells) NA_CK(cudaMemcpyAsync(scratch + o_cells, img.grid.cells.data(), b_cells, cudaMemcpyHostToDevice, c.stream));
+    if (b_cell_z) NA_CK(cudaMemcpyAsync(scratch + o_cell_z, img.grid.cell_z.data(), b_cell_z, cudaMemcpyHostToDevice, c.stream));
     if (b_entries)
         NA_CK(cudaMemcpyAsync(scratch + o_entries, img.grid.entries.data(), b_entries, cudaMemcpyHostToDevice, c.stream));
     if (b_big) NA_CK(cudaMemcpyAsync(scratch + o_big, img.grid.big.data(), b_big, cudaMemcpyHostToDevice, c.stream));

@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                 hit.tri = -1;  // the step stays inside a triangle-free z-gap: no surface to cross
                 hit.t = step;
             } else if (!(P.grid_nx > 0 &&
-                         grid_nearest(P.cells, P.cell_entries, s_big, P.n_big, P.grid_x0, P.grid_y0, P.grid_icx,
+                         grid_nearest(P.cells, P.cell_z, P.cell_entries, s_big, P.n_big, P.grid_x0, P.grid_y0, P.grid_icx,
                                       P.grid_icy, P.grid_nx, P.grid_ny, P.tris, s_tris, P.smem_tris, ph.px, ph.py, ph.pz, ph.dx,
                                       ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri, hit))) {
                 hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
@@ -596,7 +596,7 @@ extern "C" int xmc_debug_nearest(const InputInfo* in, int n_rays, const float* r
         unsigned retests = 0, nv = 0, nt = 0;
         xmc::Hit h;
         if (!(use_grid && grid.nx > 0 && tmax < INFINITY &&
-              xmc::grid_nearest(grid.cells.data(), grid.entries.data(), grid.big.data(), (int)(grid.big.size() / 4), grid.x0,
+              xmc::grid_nearest(grid.cells.data(), grid.cell_z.data(), grid.entries.data(), grid.big.data(), (int)(grid.big.size() / 4), grid.x0,
                                 grid.y0, grid.icx, grid.icy, grid.nx, grid.ny, g.tris.data(), nullptr, 0, q[0], q[1], q[2],
                                 q[3], q[4], q[5], tmin, tmax, -1, retests, nv, nt, h)))
             h = xmc::bvh_nearest(g.nodes.data(), g.tris.data(), g.n_nodes, nullptr, 0, nullptr, 0, q[0], q[1], q[2],

@@ -93,6 +93,7 @@ struct KParams {
     int n_zocc;
     // xy cell grid (grid_nx == 0: none)
     const uint2* cells;               // [grid_nx * grid_ny]: {first entry, entry count}
+    const float4* cell_z;             // [2 * grid_nx * grid_ny]: up to 4 merged z-intervals occupied in the cell
     const float4* cell_entries;       // {zmin, zmax, triangle index (bits), 0}
     const float4* big;                // [n_big * 4]: {zmin, zmax, triangle index (bits), 0}, then the 3 triangle float4s
     int n_big;
@@ -160,7 +161,7 @@ struct Context {
     void* d_nodes = nullptr; void* d_tris = nullptr; void* d_next = nullptr; void* d_dets = nullptr;
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
     void* d_counter = nullptr; void* d_status = nullptr;
-    void* d_cells = nullptr; void* d_cell_entries = nullptr; void* d_big = nullptr; void* d_cancel = nullptr;
+    void* d_cells = nullptr; void* d_cell_z = nullptr; void* d_cell_entries = nullptr; void* d_big = nullptr; void* d_cancel = nullptr;
     cudaStream_t cancel_stream = nullptr;
     void* d_scatter = nullptr; void* d_traj = nullptr; void* d_replay = nullptr; void* d_replay_count = nullptr;
     void* d_replay_ledger = nullptr;
@@ -187,6 +188,7 @@ struct GridImage {
     float x0 = 0, y0 = 0, icx = 0, icy = 0;
     int nx = 0, ny = 0;
     std::vector<uint2> cells;
+    std::vector<float4> cell_z;   // 2 per cell: (lo0, hi0, lo1, hi1), (lo2, hi2, lo3, hi3); unused = (inf, -inf)
     std::vector<float4> entries;
     std::vector<float4> big;      // 4 float4 per big triangle
 };

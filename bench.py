@@ -44,7 +44,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["heightfield", "planar"], default="heightfield")
+    p.add_argument("--workload", choices=["heightfield", "planar", "ellipsoid"], default="heightfield")
     p.add_argument("--photons", type=int, default=10_000_000)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -56,10 +56,17 @@ def make_scene(workload, photons):
     from xmcml_b200 import scenes
     if workload == "heightfield":
         return scenes.height_field_tissue(photons=photons), {
-            "workload": "heightfield-3layer-256x256-1e7", "surfaces": "2 height fields 256x256 (2x130050 tris) + 2 planes",
+            "workload": f"heightfield-3layer-256x256-{photons:.0e}", "surfaces": "2 height fields 256x256 (2x130050 tris) + 2 planes",
             "rings": 50, "time_bins": "200 x 5 ps", "roulette": "1e-4 / 0.1", "grid": "100x100x100"}
+    if workload == "ellipsoid":
+        sc = scenes.ellipsoid_target(photons=photons)
+        return sc, {
+            "workload": f"ellipsoid-target-3layer-{photons:.0e}", "surfaces": f"4 planes + icosphere ellipsoid 2x2x1 mm "
+            f"({sc.n_triangles - 8} tris) at depth 2.5", "rings": 100, "time_bins": "200 x 5 ps",
+            "grid": "256x256x128 over 20x20x10 mm", "roulette": "1e-4 / 0.1"}
     return scenes.planar(photons=photons), {
-        "workload": "planar-3layer-1e6", "rings": 50, "grid": "100x100x100 over 10x10x5 mm", "roulette": "1e-4 / 0.1"}
+        "workload": f"planar-3layer-{photons:.0e}", "rings": 50, "grid": "100x100x100 over 10x10x5 mm",
+        "roulette": "1e-4 / 0.1"}
 
 
 class ClockSampler:
@@ -329,7 +336,8 @@ def main():
             "kernel_ms_per_step": ker_ms / args.steps,
             "walk": {"steps_per_photon": last["steps"] / N, "detected_fraction": last["n_detected"] / N,
                      "fp64_retests_per_step": last["n_fp64_retests"] / max(last["steps"], 1),
-                     "escaped_top": last["escaped_top"], "absorbed": last["absorbed"]}}
+                     "escaped_top": last["escaped_top"], "absorbed": last["absorbed"],
+                     "absorbed_target": last["absorbed_target"]}}
     t.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

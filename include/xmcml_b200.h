@@ -253,6 +253,9 @@ typedef struct xmc_ledger {
     double total_ms;               /* device time of the whole run incl. zeroing and read-back  */
     uint64_t h2d_bytes;            /* bytes copied host->device for the context's device image  */
     uint64_t d2h_bytes;            /* bytes copied device->host by this run                     */
+    uint64_t absorbed_target_fx;   /* weight dropped while in a layer flagged in targetRangeLayers
+                                    * (inside or outside Area; a part of absorbed + absorbed_outside) */
+    double absorbed_target;        /* the same per launched photon                               */
 } xmc_ledger;
 
 typedef struct xmc_context xmc_context;
@@ -379,6 +382,153 @@ int xmc_debug_nearest(const InputInfo* input, int n_rays, const float* rays, flo
 /* Run the photon kernel's device-side self test: `n` Philox blocks for the given key written to
  * out[4*n] (device path), for comparing with xmc_philox4x32_10. */
 int xmc_device_philox(uint64_t seed, uint64_t photon_id, uint32_t n, uint32_t* out);
+
+/* ---------------------------------------------------------------- Part 3: batched instances
+ *
+ * Many optical-property instances of one planar layer stack in ONE persistent launch. No
+ * counterpart in the reference, which runs one InputInfo per LaunchOMP call; an instance is the
+ * planar model a caller would otherwise run through LaunchOMP: ambient medium above and below,
+ * n_layers tissue layers (planes at the cumulative thicknesses), pencil beam at normal incidence
+ * entering at the origin (or a uniform disk of beam_radius), rings of equal width around the
+ * beam axis, time bins in optical path length (the reference's timeStart/timeFinish, mm), and
+ * roulette below min_weight. Instance k walks photon ids 0..photons-1 with counter-RNG key
+ * seed_k, so it reproduces photon for photon xmc_run(seed_k) on the equivalent planar InputInfo
+ * (with XMC_ROULETTE | XMC_NO_AREA_KILL). Photon budgets may differ between instances: the
+ * kernel hands out photon ids of all instances from one dispenser. */
+#define XMC_BATCH_MAX_LAYERS 6
+#define XMC_BATCH_LEDGER 16
+
+typedef struct xmc_batch_spec {
+    uint32_t struct_size;          /* sizeof(xmc_batch_spec)                                     */
+    int32_t n_layers;              /* tissue layers, 1..XMC_BATCH_MAX_LAYERS                     */
+    int32_t n_rings;               /* ring i covers radii [i, i+1) * ring_width                  */
+    int32_t n_time;                /* time bins per ring, >= 1 (the last bin is open-ended)      */
+    double ring_width;             /* mm                                                         */
+    double time_start, time_finish;/* optical path length window of the time bins, mm            */
+    double ring_angle;             /* acceptance half-angle, degrees: -uz > cos(angle) (90 = all) */
+    double min_weight;             /* roulette threshold (e.g. 1e-4)                             */
+    double roulette_chance;        /* survival chance (e.g. 0.1)                                 */
+    uint64_t max_steps_per_photon; /* step budget per photon (0 = 1e7)                           */
+    int32_t max_instances;         /* capacity of the device tables                              */
+    int32_t use_graph;             /* 1: each run is a replayed CUDA graph; 0: plain stream work  */
+    int32_t device;
+    int32_t reserved[7];
+} xmc_batch_spec;
+
+typedef struct xmc_batch_instance {
+    double mua[XMC_BATCH_MAX_LAYERS];       /* mm^-1 */
+    double mus[XMC_BATCH_MAX_LAYERS];       /* mm^-1, mua + mus > 0 */
+    double g[XMC_BATCH_MAX_LAYERS];         /* anisotropy, (-1, 1) */
+    double n[XMC_BATCH_MAX_LAYERS];         /* refractive index */
+    double thickness[XMC_BATCH_MAX_LAYERS]; /* mm; the last tissue layer ends at the sum */
+    double n_above, n_below;                /* ambient refractive index */
+    double beam_radius;                     /* mm, uniform disk (0 = pencil beam) */
+    uint64_t photons;                       /* budget of this instance (0 allowed) */
+    uint64_t seed;                          /* counter-RNG key */
+} xmc_batch_instance;
+
+/* Launch shape of the batched kernel; chosen by xmc_batch_autotune or set by the caller. */
+typedef struct xmc_batch_tuning {
+    int32_t block_size;         /* threads per block, multiple of 32, <= 512                   */
+    int32_t blocks_per_sm;      /* resident blocks per SM (0 = as many as fit)                 */
+    int32_t photons_per_chunk;  /* photon ids a warp takes from the dispenser at a time        */
+    int32_t tally_scheme;       /* 0: per-photon global atomics for the instance ledger;
+                                 * 1: thread-private ledger sums, flushed when the thread moves
+                                 *    to another instance and at the end                      */
+    double ms;                  /* autotuner: kernel time of the winning trial                 */
+} xmc_batch_tuning;
+
+/* Per-instance ledger slots (uint64 each; *_FX are weights in 2^31 fixed point). */
+enum {
+    XMC_BL_LAUNCHED = 0, XMC_BL_STEPS = 1, XMC_BL_TOP_FX = 2, XMC_BL_BOTTOM_FX = 3, XMC_BL_ABSORBED_FX = 4,
+    XMC_BL_RKILLED_FX = 5, XMC_BL_RGAINED_FX = 6, XMC_BL_BUDGET_FX = 7, XMC_BL_N_TOP = 8, XMC_BL_N_BOTTOM = 9,
+    XMC_BL_N_ROULETTE = 10, XMC_BL_N_BUDGET = 11, XMC_BL_N_DETECTED = 12
+};
+
+/* Per-instance summary in FP64, fractions of the launched weight. */
+typedef struct xmc_batch_result {
+    uint64_t photons, steps, n_detected, n_top, n_bottom, n_roulette, n_budget;
+    double specular, escaped_top, escaped_bottom, absorbed, roulette_killed, roulette_gained, lost_budget;
+} xmc_batch_result;
+
+typedef struct xmc_batch xmc_batch;
+
+/* Host-only check of a spec and an instance table (no GPU needed): the status xmc_batch_run
+ * would return for them before touching the device. */
+int xmc_batch_validate(const xmc_batch_spec* spec, const xmc_batch_instance* inst, int n);
+
+/* Device tables for up to spec->max_instances instances on spec->device. */
+int xmc_batch_create(const xmc_batch_spec* spec, xmc_batch** out);
+
+/* Run n instances. Outputs (each may be NULL), as fractions of the instance's launched weight:
+ * ring_time[n][n_rings][n_time], ring[n][n_rings], result[n]. kernel_ms (may be NULL) gets the
+ * device time of the transport kernel. With use_graph the whole run (table upload, zeroing,
+ * kernel, FP64 reduction, read-back) is captured once per instance count and replayed. */
+int xmc_batch_run(xmc_batch* b, const xmc_batch_instance* inst, int n, double* ring_time, double* ring,
+                  xmc_batch_result* result, double* kernel_ms);
+
+/* Integer tallies of the last run: ring[n][n_rings][3] and ring_time[n][n_rings][n_time][3]
+ * as (weight_fx, count, weight^2_fx), ledger[n][XMC_BATCH_LEDGER] (XMC_BL_* slots). Any may be NULL. */
+int xmc_batch_read_tallies(xmc_batch* b, int n, uint64_t* ring, uint64_t* ring_time, uint64_t* ledger);
+
+int xmc_batch_set_tuning(xmc_batch* b, const xmc_batch_tuning* t);
+int xmc_batch_get_tuning(const xmc_batch* b, xmc_batch_tuning* t);
+
+/* Times the batched kernel on `sample` (n instances, each capped at photons_cap photons) for
+ * every candidate launch shape (block size x blocks per SM x photons per chunk x tally scheme),
+ * keeps the fastest in `b` and returns it in *best. */
+int xmc_batch_autotune(xmc_batch* b, const xmc_batch_instance* sample, int n, uint64_t photons_cap,
+                       xmc_batch_tuning* best);
+
+int xmc_batch_destroy(xmc_batch* b);
+
+/* ---------------------------------------------------------------- Part 4: surrogate network
+ *
+ * A fully connected network (n_hidden SiLU layers of width `hidden`, linear output) trained and
+ * evaluated on the GPU's tensor cores: BF16 weights and activations, FP32 accumulation, FP32
+ * master weights and Adam moments. No counterpart in the reference. It stands in for the Monte
+ * Carlo inside inverse fitting: inputs are optical properties of a layered model, outputs its
+ * ring- and time-resolved reflectance (the caller's normalisation on both sides). Row counts of
+ * every call are multiples of 128 up to max_rows. Calls on one model are serialised. */
+typedef struct xmc_mlp_spec {
+    uint32_t struct_size;   /* sizeof(xmc_mlp_spec)                           */
+    int32_t n_in;           /* inputs, 1..64                                  */
+    int32_t hidden;         /* hidden width: 128 or 256                       */
+    int32_t n_hidden;       /* hidden layers, 1..8                            */
+    int32_t n_out;          /* outputs, 1..4096                               */
+    int32_t max_rows;       /* row capacity of a forward or training batch    */
+    int32_t device;
+    int32_t reserved[9];
+} xmc_mlp_spec;
+
+typedef struct xmc_mlp xmc_mlp;
+
+int xmc_mlp_create(const xmc_mlp_spec* spec, xmc_mlp** out);
+/* Number of FP32 parameters in the flat layout: for each layer l, W_l [out_l][in_l] row-major
+ * then b_l [out_l] (in_0 = n_in, out_last = n_out). */
+int64_t xmc_mlp_param_count(const xmc_mlp* m);
+/* Set / get the FP32 master parameters (set also resets the Adam moments and step count). */
+int xmc_mlp_set_params(xmc_mlp* m, const float* params);
+int xmc_mlp_get_params(const xmc_mlp* m, float* params);
+/* y[rows][n_out] = network(x[rows][n_in]) with host buffers; *ms (may be NULL) = device time. */
+int xmc_mlp_forward(xmc_mlp* m, const float* x, int rows, float* y, double* ms);
+/* Mean device time of `reps` forward passes over the inputs of the last xmc_mlp_forward call
+ * (device-resident, replayed CUDA graph). */
+int xmc_mlp_forward_timed(xmc_mlp* m, int rows, int reps, double* ms);
+/* Gradients of the mean squared error over rows (flat parameter layout), no update. */
+int xmc_mlp_gradients(xmc_mlp* m, const float* x, const float* t, int rows, float* grads, float* loss);
+/* Device-resident training set x[rows][n_in], t[rows][n_out]. */
+int xmc_mlp_set_dataset(xmc_mlp* m, const float* x, const float* t, int rows);
+/* `steps` Adam steps on minibatches of `batch` rows drawn from the training set with replacement
+ * (Philox keyed by seed); losses[steps] (may be NULL) = each minibatch's mean squared error. */
+int xmc_mlp_train(xmc_mlp* m, int steps, int batch, float lr, float beta1, float beta2, float eps,
+                  uint64_t seed, float* losses, double* ms);
+int xmc_mlp_destroy(xmc_mlp* m);
+
+/* D[M][N] = A[M][K] . B[N][K]^T on the tensor cores (bf16 inputs as raw 16-bit patterns, FP32
+ * out) through the network's GEMM kernel, tile width bn (64, 128, 256) and `splits` K-splits;
+ * M % 128, N % bn and K % (64 splits) must be 0. For tests. */
+int xmc_gemm_bf16(const uint16_t* a, const uint16_t* b, int M, int N, int K, int bn, int splits, float* d);
 
 #ifdef __cplusplus
 }

@@ -38,7 +38,7 @@ _TERMS = ["specular", "absorbed", "absorbed_outside", "escaped_top", "escaped_bo
 
 
 class OracleLedger(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in _CNT] + [(n, C.c_double) for n in _TERMS]
+    _fields_ = [(n, C.c_uint64) for n in _CNT] + [(n, C.c_double) for n in _TERMS] + [("absorbed_target", C.c_double)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -66,6 +66,7 @@ typedef struct oracle_ledger {
         n_invalid, n_detected;
     double specular, absorbed, absorbed_outside, escaped_top, escaped_bottom, lost_area, lost_cut,
         lost_glass, lost_budget, lost_invalid, roulette_killed, roulette_gained;
+    double absorbed_target; /* weight dropped in layers flagged in targetRangeLayers (inside or outside Area) */
 } oracle_ledger;
 
 /* ------------------------------------------------------------------------ RNG: MCG59 */
@@ -698,6 +699,7 @@ static void o_absorb_outside(o_out* po, o_photon* ph, const InputInfo* in) {
     double dw = ph->weight * L->absorptionCoefficient / (L->absorptionCoefficient + L->scatteringCoefficient);
     ph->weight -= dw;
     po->led.absorbed_outside += dw;
+    if (in->targetRangeLayers[ph->layer]) po->led.absorbed_target += dw;
 }
 
 /* mcml_kernel.cpp:39-126: one photon, start to death */
@@ -754,6 +756,7 @@ static void o_photon_walk(const o_ctx* C, o_out* po, o_rng* rng, o_traj* tr) {
                         ph.weight -= dw;
                         po->absorption[idx] += dw;
                         po->led.absorbed += dw;
+                        if (in->targetRangeLayers[ph.layer]) po->led.absorbed_target += dw;
                     } else {
                         o_absorb_outside(po, &ph, in);
                     }
@@ -806,6 +809,7 @@ static void o_led_add(oracle_ledger* a, const oracle_ledger* b) {
     a->lost_area += b->lost_area; a->lost_cut += b->lost_cut; a->lost_glass += b->lost_glass;
     a->lost_budget += b->lost_budget; a->lost_invalid += b->lost_invalid;
     a->roulette_killed += b->roulette_killed; a->roulette_gained += b->roulette_gained;
+    a->absorbed_target += b->absorbed_target;
 }
 
 void oracle_default_opts(oracle_opts* o) {

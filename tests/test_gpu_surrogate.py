@@ -1,0 +1,128 @@
+"""Tensor-core kernels of the surrogate network against the numpy oracle (oracle/mlp_ref.py).
+
+  * the tcgen05 GEMM (TMA, TMEM accumulator) on every tile width and with split-K, exact up to
+    FP32 accumulation order;
+  * the forward pass (bias, SiLU, BF16 activations) and the gradients of the mean squared error
+    against the oracle's FP64 back-propagation with the same BF16 roundings;
+  * one training step (minibatch gather, forward, backward, Adam) against the oracle's Adam step
+    on the same rows, and that training lowers the loss.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import mlp_ref as R
+from xmcml_b200 import _lib
+from xmcml_b200 import surrogate as SG
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("M,N,K,bn,splits", [(128, 64, 64, 64, 1), (256, 256, 256, 256, 1), (384, 128, 512, 128, 1),
+                                             (128, 1024, 256, 256, 1), (256, 256, 2048, 256, 4), (512, 64, 1024, 64, 8),
+                                             (128, 256, 64 * 37, 256, 1)])
+def test_gemm_matches_numpy(M, N, K, bn, splits):
+    rng = np.random.default_rng(M * 7 + N + K)
+    a = SG.to_bf16_bits(rng.standard_normal((M, K)).astype(np.float32))
+    b = SG.to_bf16_bits(rng.standard_normal((N, K)).astype(np.float32))
+    d = SG.gemm_bf16(a, b, bn=bn, splits=splits)
+    ref = SG.from_bf16_bits(a).astype(np.float64) @ SG.from_bf16_bits(b).astype(np.float64).T
+    err = np.abs(d - ref).max() / np.abs(ref).max()
+    print(f"gemm {M}x{N}x{K} bn {bn} splits {splits}: max rel err {err:.2e}")
+    assert err < 1e-5
+
+
+DIMS = dict(n_in=15, hidden=256, n_hidden=4, n_out=1000)
+
+
+def _model_and_params(seed=0, max_rows=1024):
+    rng = np.random.default_rng(seed)
+    p = R.init_params(rng, DIMS["n_in"], DIMS["hidden"], DIMS["n_hidden"], DIMS["n_out"])
+    p[-DIMS["n_out"]:] = rng.normal(0, 0.1, DIMS["n_out"])  # non-zero output bias
+    m = SG.MLP(DIMS["n_in"], DIMS["n_out"], DIMS["hidden"], DIMS["n_hidden"], max_rows=max_rows)
+    m.set_params(p)
+    return m, p, rng
+
+
+def test_forward_matches_oracle():
+    m, p, rng = _model_and_params(1)
+    assert m.n_params == p.size == 15 * 256 + 256 + 3 * (256 * 256 + 256) + 256 * 1000 + 1000
+    assert np.array_equal(m.get_params(), p)
+    x = rng.standard_normal((300, 15)).astype(np.float32)  # 300 rows: padded to 384 inside
+    y, ms = m.forward(x)
+    ref = R.forward(p, x, **DIMS)
+    err = np.abs(y - ref).max() / np.abs(ref).max()
+    print(f"forward max rel err {err:.2e} ({ms:.3f} ms)")
+    assert err < 2e-2
+    assert np.median(np.abs(y - ref)) / np.abs(ref).mean() < 2e-3
+    m.close()
+
+
+def test_gradients_match_oracle():
+    m, p, rng = _model_and_params(2)
+    x = rng.standard_normal((512, 15)).astype(np.float32)
+    t = (R.forward(p, x, **DIMS) + rng.normal(0, 0.5, (512, 1000))).astype(np.float32)
+    g, loss = m.gradients(x, t)
+    gr, lr_ = R.gradients(p, x, t, **DIMS)
+    assert loss == pytest.approx(lr_, rel=1e-3)
+    o = 0
+    for i, (r, c) in enumerate(R.shapes(15, 256, 4, 1000)):
+        for name, sz in (("W", r * c), ("b", r)):
+            gg, rr = g[o:o + sz].astype(np.float64), gr[o:o + sz]
+            o += sz
+            rel = np.linalg.norm(gg - rr) / np.linalg.norm(rr)
+            cos = gg @ rr / (np.linalg.norm(gg) * np.linalg.norm(rr))
+            print(f"layer {i} {name}: rel err {rel:.2e} cosine {cos:.6f}")
+            assert rel < 2e-2 and cos > 0.9998
+    m.close()
+
+
+def _philox_rows(seed, step, batch, ds_rows):
+    lib = _lib.load()
+    key = (C.c_uint32 * 2)(seed & 0xffffffff, seed >> 32)
+    out = (C.c_uint32 * 4)()
+    rows = []
+    for r in range(batch):
+        ctr = (C.c_uint32 * 4)(r, step, 0x6d6c70, 0)
+        lib.xmc_philox4x32_10(ctr, key, out)
+        rows.append((out[0] * ds_rows) >> 32)
+    return np.array(rows)
+
+
+def test_training_step_matches_oracle_adam():
+    m, p, rng = _model_and_params(3)
+    ds = 1000
+    x = rng.standard_normal((ds, 15)).astype(np.float32)
+    t = (np.tanh(x @ rng.standard_normal((15, 1000)) * 0.3)).astype(np.float32)
+    m.set_dataset(x, t)
+    seed, batch, lr = 12345, 256, 1e-3
+    losses, ms = m.train(1, batch=batch, lr=lr, seed=seed)
+    idx = _philox_rows(seed, 1, batch, ds)
+    g, loss = R.gradients(p, x[idx], t[idx], **DIMS)
+    assert losses[0] == pytest.approx(loss, rel=1e-3)
+    pn, _, _ = R.adam_step(p.astype(np.float64), g, np.zeros_like(g), np.zeros_like(g), 1, lr)
+    got = m.get_params().astype(np.float64)
+    # first Adam step moves every parameter with a non-negligible gradient by about lr
+    dp_ref, dp = pn - p, got - p
+    big = np.abs(g) > 1e-6 * np.abs(g).max()
+    agree = np.mean(np.abs(dp[big] - dp_ref[big]) < 0.05 * lr)
+    print(f"adam step: {agree:.4f} of parameters within 5% of lr, loss {losses[0]:.5f} vs {loss:.5f}")
+    assert agree > 0.98
+    m.close()
+
+
+def test_training_lowers_the_loss():
+    m, p, rng = _model_and_params(4, max_rows=2048)
+    ds = 8192
+    x = rng.standard_normal((ds, 15)).astype(np.float32)
+    w = rng.standard_normal((15, 1000)) * 0.3
+    t = np.tanh(x @ w).astype(np.float32)
+    m.set_dataset(x, t)
+    losses, ms = m.train(300, batch=1024, lr=1e-3, seed=7)
+    print(f"loss {losses[:5].mean():.4f} -> {losses[-5:].mean():.4f} in {ms:.1f} ms")
+    assert np.all(np.isfinite(losses))
+    assert losses[-20:].mean() < 0.3 * losses[:5].mean()
+    y, _ = m.forward(x[:512])
+    assert np.mean((y - t[:512]) ** 2) < 0.5 * losses[:5].mean()
+    m.close()

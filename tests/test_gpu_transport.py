@@ -126,6 +126,27 @@ def test_height_field_rings_and_time_bins(tmp_path):
     assert np.all(np.abs(z) < 3.0)
 
 
+def test_ellipsoid_target_region(tmp_path):
+    """Large target-region scene (3 planar layers + a triangulated ellipsoid inside L3, absorption grid
+    256x256x128, 100 rings x 200 time bins), at 20,480 triangles: rings, time bins, ledger and the
+    weight absorbed inside the target."""
+    n = 100_000
+    sc = scenes.ellipsoid_target(photons=n, subdiv=5)
+    m, led, tal, out, oled, dw2, tw2 = _run_pair(tmp_path, sc, n, roulette=True)
+    _check_exact(led, n)
+    assert led["n_invalid"] == 0
+    _check_rings(tal, out, dw2, n, "ellipsoid")
+    _check_ledger_terms(led, oled, n, "ellipsoid")
+    g = led["absorbed_target_fx"] / WEIGHT_SCALE
+    o = oled["absorbed_target"]
+    print(f"ellipsoid: absorbed in target gpu {g / n:.6f} oracle {o / n:.6f}")
+    assert o > 0.0 and abs(g - o) / np.sqrt(g + o) < 3.0
+    g = tal["time_weight"].astype(float) / WEIGHT_SCALE
+    z = zscores(g, out.time_weights(), sum_var(g, tal["time_weight2"].astype(float) / WEIGHT_SCALE, n),
+                sum_var(out.time_weights(), tw2, n))
+    assert np.all(np.abs(z) < 3.0)
+
+
 def test_glass_cubes_filters_targets_beam(tmp_path):
     n = 100_000
     sc = rich_planar(n)

@@ -61,6 +61,28 @@ def load(path: str | None = None) -> C.CDLL:
                                         P(C.c_float), P(C.c_int), P(C.c_float), C.c_int]),
         "xmc_run_noalloc": (C.c_int, [P(S.InputInfo), P(S.XmcOptions), C.c_uint64, C.c_uint64, C.c_uint64,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "xmc_batch_validate": (C.c_int, [P(S.BatchSpec), P(S.BatchInstance), C.c_int]),
+        "xmc_batch_create": (C.c_int, [P(S.BatchSpec), P(C.c_void_p)]),
+        "xmc_batch_run": (C.c_int, [C.c_void_p, P(S.BatchInstance), C.c_int, P(C.c_double), P(C.c_double),
+                                    P(S.BatchResult), P(C.c_double)]),
+        "xmc_batch_read_tallies": (C.c_int, [C.c_void_p, C.c_int, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+        "xmc_batch_set_tuning": (C.c_int, [C.c_void_p, P(S.BatchTuning)]),
+        "xmc_batch_get_tuning": (C.c_int, [C.c_void_p, P(S.BatchTuning)]),
+        "xmc_batch_autotune": (C.c_int, [C.c_void_p, P(S.BatchInstance), C.c_int, C.c_uint64, P(S.BatchTuning)]),
+        "xmc_batch_destroy": (C.c_int, [C.c_void_p]),
+        "xmc_mlp_create": (C.c_int, [P(S.MlpSpec), P(C.c_void_p)]),
+        "xmc_mlp_param_count": (C.c_int64, [C.c_void_p]),
+        "xmc_mlp_set_params": (C.c_int, [C.c_void_p, P(C.c_float)]),
+        "xmc_mlp_get_params": (C.c_int, [C.c_void_p, P(C.c_float)]),
+        "xmc_mlp_forward": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int, P(C.c_float), P(C.c_double)]),
+        "xmc_mlp_forward_timed": (C.c_int, [C.c_void_p, C.c_int, C.c_int, P(C.c_double)]),
+        "xmc_mlp_gradients": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_int, P(C.c_float), P(C.c_float)]),
+        "xmc_mlp_set_dataset": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_int]),
+        "xmc_mlp_train": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                    C.c_uint64, P(C.c_float), P(C.c_double)]),
+        "xmc_mlp_destroy": (C.c_int, [C.c_void_p]),
+        "xmc_gemm_bf16": (C.c_int, [P(C.c_uint16), P(C.c_uint16), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -87,4 +109,9 @@ EXPORTS = [
     "xmc_parse_input_file", "xmc_parse_surface_file", "xmc_free_input", "xmc_write_output_file",
     "xmc_specular_reflectance", "xmc_philox4x32_10", "xmc_layout_offsets", "xmc_device_philox",
     "xmc_generate_bvh_tree", "xmc_free_bvh_tree", "xmc_debug_nearest", "xmc_run_noalloc",
+    "xmc_batch_validate", "xmc_batch_create", "xmc_batch_run", "xmc_batch_read_tallies", "xmc_batch_set_tuning",
+    "xmc_batch_get_tuning", "xmc_batch_autotune", "xmc_batch_destroy",
+    "xmc_mlp_create", "xmc_mlp_param_count", "xmc_mlp_set_params", "xmc_mlp_get_params", "xmc_mlp_forward",
+    "xmc_mlp_forward_timed", "xmc_mlp_gradients", "xmc_mlp_set_dataset", "xmc_mlp_train", "xmc_mlp_destroy",
+    "xmc_gemm_bf16",
 ]

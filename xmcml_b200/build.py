@@ -18,8 +18,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libxmcml_b200.so")
 
-SOURCES = ["transport.cu", "noalloc.cu", "capi.cpp", "io.cpp", "bvh.cpp"]
-HEADERS = ["xmc_internal.h", "geom.cuh"]
+SOURCES = ["transport.cu", "batch.cu", "surrogate.cu", "noalloc.cu", "capi.cpp", "io.cpp", "bvh.cpp"]
+HEADERS = ["xmc_internal.h", "geom.cuh", "photon.cuh", "tc_gemm.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -323,6 +323,8 @@ void fill_ledger(const unsigned long long* L, uint32_t w0_fx, uint64_t n, xmc_le
     led->lost_invalid = (double)led->lost_invalid_fx * s;
     led->roulette_killed = (double)led->roulette_killed_fx * s;
     led->roulette_gained = (double)led->roulette_gained_fx * s;
+    led->absorbed_target_fx = L[L_ABSORBED_TGT];
+    led->absorbed_target = (double)led->absorbed_target_fx * s;
 }
 
 static int create(const InputInfo* in, const xmc_options* opt_in, Context** out) {

@@ -18,6 +18,7 @@
 #include <cstdint>
 
 #include "geom.cuh"
+#include "photon.cuh"
 #include "xmc_internal.h"
 
 namespace xmc {
@@ -25,21 +26,6 @@ namespace xmc {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-    return c;
-}
-
-// 24-bit uniform in (0,1), exactly the value the FP64 oracle uses.
-__device__ __forceinline__ float u24(uint32_t x) { return fmaf((float)(x >> 8), 0x1p-24f, 0x1p-25f); }
 
 struct Photon {
     float px, py, pz, dx, dy, dz;
@@ -267,7 +253,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     bool alive = false;
     Photon ph;
     unsigned steps = 0, retests = 0, n_visit = 0, n_tri = 0;
-    unsigned long long absorbed = 0, absorbed_out = 0;  // per-thread sums, flushed once at the end
+    unsigned long long absorbed = 0, absorbed_out = 0, absorbed_tgt = 0;  // per-thread sums, flushed at the end
     unsigned budget_hit = 0;
 
     for (;;) {
@@ -390,47 +376,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             }
             const float ni = L.n, nt = s_layer[next].n;
             const float dn = ph.dx * nx + ph.dy * ny + ph.dz * nz;
-            const float ci = fabsf(dn);
-            float R;
-            if (ni == nt) {
-                R = 0.0f;
-            } else {
-                // GetCriticalCos (mcml_kernel.cpp:644-661)
-                const float cc = ni > nt ? sqrtf(1.0f - (nt * nt) / (ni * ni)) : 0.0f;
-                if (ci <= cc) {
-                    R = 1.0f;
-                } else if (ci > 1.0f - 1e-6f) {
-                    R = (nt - ni) / (nt + ni);
-                    R *= R;
-                } else if (ci < 1e-6f) {
-                    R = 1.0f;
-                } else if (ni > nt && ci - cc < 1e-3f) {
-                    // near the critical angle: ComputeTransmitCosine + ComputeFrenselReflectance in FP64
-                    const double Ci = ci, Ni = ni, Nt = nt;
-                    const double Si = sqrt(1.0 - Ci * Ci);
-                    const double St = Ni * Si / Nt;
-                    if (St >= 1.0) {
-                        R = 1.0f;
-                    } else {
-                        const double Ct = sqrt(1.0 - St * St);
-                        const double cs = Ci * Ct - Si * St, cd = Ci * Ct + Si * St;
-                        const double ss = Si * Ct + Ci * St, sd = Si * Ct - Ci * St;
-                        R = (float)(0.5 * sd * sd * (cd * cd + cs * cs) / (ss * ss * cd * cd));
-                    }
-                } else {
-                    // ComputeTransmitCosine / ComputeFrenselReflectance (mcml_kernel.cpp:497-564)
-                    const float si = sqrtf(1.0f - ci * ci);
-                    const float st = ni * si / nt;
-                    if (st >= 1.0f) {
-                        R = 1.0f;
-                    } else {
-                        const float ct = sqrtf(1.0f - st * st);
-                        const float cs = ci * ct - si * st, cd = ci * ct + si * st;
-                        const float ss = si * ct + ci * st, sd = si * ct - ci * st;
-                        R = 0.5f * sd * sd * (cd * cd + cs * cs) / (ss * ss * cd * cd);
-                    }
-                }
-            }
+            const float R = fresnel_reflectance(ni, nt, fabsf(dn));
             const float u_fresnel = L.glass ? u24(r.x) : u24(r.y);
             if (u_fresnel > R) {
                 if (next == 0) {
@@ -482,37 +428,9 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             } else {
                 absorbed_out += dw;
             }
+            if ((P.target_mask >> ph.layer) & 1u) absorbed_tgt += dw;
             // ---- spin (mcml_kernel.cpp:442-495) ----
-            const float u1 = u24(r.y);
-            float cost;
-            if (L.g != 0.0f) {
-                const float t = L.hg_a / (L.hg_d + L.hg_e * u1);
-                cost = (L.hg_b - t * t) * L.hg_c;
-            } else {
-                cost = 2.0f * u1 - 1.0f;
-            }
-            cost = fminf(1.0f, fmaxf(-1.0f, cost));
-            const float sint = sqrtf(fmaxf(0.0f, 1.0f - cost * cost));
-            float a = u24(r.z);
-            a = a > 0.5f ? a - 1.0f : a;  // same angle as 2*pi*u, reduced to [-pi, pi]
-            float sp, cp;
-            __sincosf(6.283185307179586f * a, &sp, &cp);
-            const float ux = ph.dx, uy = ph.dy, uz = ph.dz;
-            const float rho2 = ux * ux + uy * uy;
-            float nx, ny, nz;
-            if (rho2 > 1e-12f) {
-                const float irho = rsqrtf(rho2);
-                const float rho = rho2 * irho;
-                nx = sint * (ux * uz * cp - uy * sp) * irho + ux * cost;
-                ny = sint * (uy * uz * cp + ux * sp) * irho + uy * cost;
-                nz = -sint * cp * rho + uz * cost;
-            } else {
-                nx = sint * cp;
-                ny = sint * sp;
-                nz = uz >= 0.0f ? cost : -cost;
-            }
-            const float on = rsqrtf(nx * nx + ny * ny + nz * nz);
-            ph.dx = nx * on; ph.dy = ny * on; ph.dz = nz * on;
+            hg_spin(L.hg_a, L.hg_b, L.hg_c, L.hg_d, L.hg_e, u24(r.y), u24(r.z), ph.dx, ph.dy, ph.dz);
             ph.excl = -1;
             ph.tmin = 0.0f;
         }
@@ -538,6 +456,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     atomicAdd(&S.ledger[L_STEPS], (unsigned long long)steps);
     lat(&S.ledger[L_ABSORBED], absorbed);
     lat(&S.ledger[L_ABSORBED_OUT], absorbed_out);
+    lat(&S.ledger[L_ABSORBED_TGT], absorbed_tgt);
     if (retests) atomicAdd(&S.ledger[L_N_RETEST], (unsigned long long)retests);
     atomicAdd(&S.ledger[L_N_NODES], (unsigned long long)n_visit);
     atomicAdd(&S.ledger[L_N_TRIS], (unsigned long long)n_tri);

@@ -63,7 +63,7 @@ enum LedgerSlot {
     L_N_TOP, L_N_BOTTOM, L_N_AREA, L_N_CUT, L_N_ROULETTE, L_N_GLASS, L_N_BUDGET, L_N_INVALID,
     L_N_DETECTED, L_N_RETEST, L_N_NODES, L_N_TRIS,
     L_ABSORBED, L_ABSORBED_OUT, L_TOP, L_BOTTOM, L_AREA, L_CUT, L_GLASS, L_BUDGET, L_INVALID,
-    L_RKILLED, L_RGAINED, L_N_REPLAY_MISMATCH,
+    L_RKILLED, L_RGAINED, L_N_REPLAY_MISMATCH, L_ABSORBED_TGT,
     L_COUNT
 };
 constexpr int kLedgerSlots = 32;  // padded

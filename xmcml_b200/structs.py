@@ -138,7 +138,53 @@ class XmcLedger(C.Structure):
                 + [(n + "_fx", C.c_uint64) for n in LEDGER_TERMS]
                 + [(n, C.c_double) for n in LEDGER_TERMS]
                 + [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_uint64),
-                   ("d2h_bytes", C.c_uint64)])
+                   ("d2h_bytes", C.c_uint64), ("absorbed_target_fx", C.c_uint64), ("absorbed_target", C.c_double)])
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+# ----------------------------------------------------------------------------- batched instances
+
+XMC_BATCH_MAX_LAYERS = 6
+XMC_BATCH_LEDGER = 16
+BATCH_LEDGER_SLOTS = ["launched", "steps", "top_fx", "bottom_fx", "absorbed_fx", "rkilled_fx", "rgained_fx",
+                      "budget_fx", "n_top", "n_bottom", "n_roulette", "n_budget", "n_detected"]
+
+
+class BatchSpec(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("n_layers", C.c_int32), ("n_rings", C.c_int32), ("n_time", C.c_int32),
+                ("ring_width", C.c_double), ("time_start", C.c_double), ("time_finish", C.c_double),
+                ("ring_angle", C.c_double), ("min_weight", C.c_double), ("roulette_chance", C.c_double),
+                ("max_steps_per_photon", C.c_uint64), ("max_instances", C.c_int32), ("use_graph", C.c_int32),
+                ("device", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+_L6 = C.c_double * XMC_BATCH_MAX_LAYERS
+
+
+class BatchInstance(C.Structure):
+    _fields_ = [("mua", _L6), ("mus", _L6), ("g", _L6), ("n", _L6), ("thickness", _L6), ("n_above", C.c_double),
+                ("n_below", C.c_double), ("beam_radius", C.c_double), ("photons", C.c_uint64), ("seed", C.c_uint64)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("photons_per_chunk", C.c_int32),
+                ("tally_scheme", C.c_int32), ("ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class BatchResult(C.Structure):
+    _fields_ = ([(n, C.c_uint64) for n in ["photons", "steps", "n_detected", "n_top", "n_bottom", "n_roulette",
+                                           "n_budget"]]
+                + [(n, C.c_double) for n in ["specular", "escaped_top", "escaped_bottom", "absorbed",
+                                             "roulette_killed", "roulette_gained", "lost_budget"]])
+
+
+# ----------------------------------------------------------------------------- surrogate network
+
+class MlpSpec(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("n_in", C.c_int32), ("hidden", C.c_int32), ("n_hidden", C.c_int32),
+                ("n_out", C.c_int32), ("max_rows", C.c_int32), ("device", C.c_int32), ("reserved", C.c_int32 * 9)]

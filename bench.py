@@ -49,6 +49,7 @@ def parse_args():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-surrogate", action="store_true")
     return p.parse_args()
 
 
@@ -243,6 +244,51 @@ def roofline(led, kernel_ms, clocks, n_photons):
                                      "has no SIMT figure; the walk is not HBM- or tensor-bound)"}}
 
 
+def surrogate_inference(local):
+    """Surrogate evals/s: the 15 -> 256 x 4 (SiLU) -> 1000 network (random He-uniform weights: the
+    speed does not depend on their values) on a 65,536-row batch on the tensor cores; device time of
+    the resident forward pass (CUDA graph of the five GEMMs) and host-to-host time of one call."""
+    import numpy as np
+    from xmcml_b200 import surrogate as SG
+    rows = 65536
+    m = SG.MLP(15, 1000, 256, 4, max_rows=rows, device=local)
+    m.set_params(SG.he_uniform(np.random.default_rng(0), 15, 256, 4, 1000))
+    x = np.random.default_rng(1).standard_normal((rows, 15)).astype(np.float32)
+    m.forward(x)
+    t0 = time.perf_counter()
+    m.forward(x)
+    e2e_s = time.perf_counter() - t0
+    ms = m.forward_timed(rows, reps=50)
+    m.close()
+    algo = 2.0 * rows * (15 * 256 + 3 * 256 * 256 + 256 * 1000)   # multiply-adds of the network x 2
+    issued = 2.0 * rows * (64 * 256 + 3 * 256 * 256 + 256 * 1024)  # with the padded input / output tiles
+    peak = None
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
+    except Exception:
+        pass
+    evals = rows / (ms / 1e3)
+    # the Monte Carlo the network stands in for: batched planar 3-layer instances on this GPU
+    from xmcml_b200 import batch as XB
+    b = XB.Batch(device=local, max_instances=64)
+    inst = XB.sample_instances(3, 64, budget=(1e6, 1e6))
+    b.run(inst.with_photons(20000))
+    mc = b.run(inst)
+    b.close()
+    mc_rate = float(inst.photons.sum()) / (mc["kernel_ms"] / 1e3)
+    mc_evals = mc_rate / 1e7
+    return {"metric": "surrogate evals/s", "value": evals, "batch": rows, "ms_per_batch": ms,
+            "e2e": {"value": rows / e2e_s, "unit": "evals/s", "h2d_bytes_per_step": rows * 15 * 4,
+                    "d2h_bytes_per_step": rows * 1000 * 4},
+            "roofline": {"bound": "tensor", "achieved": algo / (ms / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (algo / (ms / 1e3) / 1e12 / peak) if peak else None,
+                         "issued_tflops": issued / (ms / 1e3) / 1e12,
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS 8192^3)"},
+            "vs_mc_1e7_photon_evals": evals / mc_evals, "mc_evals_per_s_at_1e7_photons": mc_evals,
+            "mc_batched_photons_per_s": mc_rate,
+            "error_note": "accuracy of the trained ensemble is measured by xmcml_b200.surrogate_study, not here"}
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -301,6 +347,13 @@ def main():
         e2e = run_e2e(args, m, N, rank, local, world, barrier, dist, torch)
     line_e2e = e2e
 
+    sur = None
+    if not args.no_surrogate:
+        try:
+            sur = surrogate_inference(local)
+        except Exception as e:  # reported, not fatal
+            sur = {"metric": "surrogate evals/s", "value": None, "error": str(e)}
+
     rl = roofline(last, last["kernel_ms"], clocks, N)
     prof = os.path.join(ROOT, "profiles", f"transport_kernel_{args.workload}_dram.json")
     if os.path.exists(prof):
@@ -332,7 +385,7 @@ def main():
             "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "config": cfg, "clocks": clocks,
             "e2e": line_e2e,
-            "gpu_launches": args.steps, "roofline": rl, "cpu_baseline": cpu,
+            "gpu_launches": args.steps, "roofline": rl, "cpu_baseline": cpu, "surrogate": sur,
             "kernel_ms_per_step": ker_ms / args.steps,
             "walk": {"steps_per_photon": last["steps"] / N, "detected_fraction": last["n_detected"] / N,
                      "fp64_retests_per_step": last["n_fp64_retests"] / max(last["steps"], 1),

@@ -91,6 +91,21 @@ def test_kernel_query_matches_oracle(tmp_path, name, tmax, use_grid):
     assert np.all(np.abs(np.abs(np.sum(nrm[hit] * on[hit], 1)) - 1) < 1e-4)
 
 
+@pytest.mark.parametrize("tmax", [0.3, 5.0])
+def test_queries_outside_the_cell_grid(tmp_path, tmax):
+    """The cell grid covers the small triangles only (here the ellipsoid, 4 x 4 mm); the layer planes
+    (+-100 mm) are tested from the large-triangle list, also for segments outside the grid."""
+    xml, surf = scenes.ellipsoid_target(photons=1, subdiv=4).write(str(tmp_path), "e")
+    m = api.Model(xml, surf)
+    r = rays(1500, 31, lo=(-40, -40, -0.2), hi=(40, 40, 4))
+    r[:500, 2] = np.random.default_rng(5).uniform(-0.08, 0.2, 500)
+    t, s, _ = kernel_query(m.info, r, tmax, use_grid=1)
+    ot, os_, _ = oracle_query(m.info, r, tmax)
+    ok = agree(t, s, ot, os_)
+    assert ok.mean() >= 0.999, f"{(~ok).sum()} disagreements"
+    assert (os_ >= 0).sum() > 50
+
+
 @pytest.mark.skipif(not B.ref_available(), reason="reference build oracle/_ref missing")
 @pytest.mark.parametrize("name", list(SCENES))
 def test_kernel_query_matches_reference_bvh_and_converted_tree(tmp_path, name):

@@ -126,3 +126,48 @@ def test_training_lowers_the_loss():
     y, _ = m.forward(x[:512])
     assert np.mean((y - t[:512]) ** 2) < 0.5 * losses[:5].mean()
     m.close()
+
+
+def test_surrogate_beats_equal_cost_monte_carlo():
+    """What the trained network gains: trained on batched-MC tallies of sampled 3-layer instances, it
+    predicts the ring x time reflectance of held-out instances more accurately than a Monte Carlo
+    run given the same GPU time per instance, and its ensemble gate and training hull route the
+    rest to the Monte Carlo."""
+    import time
+    from xmcml_b200 import batch as XB
+
+    rings, times = 10, 4
+    b = XB.Batch(n_rings=rings, n_time=times, ring_width=0.2, time_finish=1000 * 0.299792458, max_instances=4096)
+    train = XB.sample_instances(101, 3000, budget=(20000, 20000))
+    out = b.run(train)
+    ytr = SG.reflectance_targets(out["ring_time"], floor=1e-6)
+    test = XB.sample_instances(202, 64, budget=(2_000_000, 2_000_000))
+    ref = b.run(test)
+    tal = b.tallies()
+    w2 = tal["ring_time"][:, :, :, 2].astype(np.float64) / 2 ** 31  # sum of squared weights per cell
+    sur = SG.Surrogate(n_in=15, n_out=rings * times, members=2, max_rows=4096, floor=1e-6, gate=1.0)
+    curves = sur.fit(train.features(), ytr, steps=1500, batch=1024, lr=2e-3)
+    assert all(c[-50:].mean() < 0.2 * c[:10].mean() for c in curves)
+    t0 = time.perf_counter()
+    pred = sur.predict(test.features())
+    t_net = (time.perf_counter() - t0) / len(test)
+    e_net = SG.relative_error(pred["log10_r"], ref["ring_time"], w2, test.photons, floor=1e-6, max_ref_rse=0.02)
+    # a Monte Carlo run per instance with the network's wall time per instance, at this GPU's rate
+    rate = float(test.photons.sum()) / (ref["kernel_ms"] / 1e3)
+    n_mc = max(1, int(rate * t_net))
+    mc = b.run(test.with_photons(n_mc))
+    e_mc = SG.relative_error(np.log10(mc["ring_time"].reshape(len(test), -1) + 1e-6), ref["ring_time"], w2,
+                             test.photons, floor=1e-6, max_ref_rse=0.02)
+    med_net, med_mc = np.nanmedian(e_net), np.nanmedian(e_mc)
+    print(f"median relative error: network {med_net:.4f}, MC at equal time ({n_mc} photons) {med_mc:.4f}; "
+          f"network {t_net * 1e6:.1f} us/instance incl. host, {np.isfinite(e_net).mean():.2f} of cells judged")
+    assert med_net < 0.1
+    assert med_net < med_mc
+    # gate and hull: outside the training distribution the answer comes from the Monte Carlo
+    odd = test.subset(range(4))
+    odd.mus[:, 0] = 80.0  # outside [5, 40]
+    res = sur.reflectance(odd, batch=b, fallback_photons=20000)
+    assert not res["from_network"].any()
+    assert np.all(np.isfinite(res["reflectance"]))
+    sur.close()
+    b.close()

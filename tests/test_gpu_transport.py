@@ -323,3 +323,34 @@ def test_zero_photons_and_no_detectors(tmp_path):
     led = t.run(1000)
     assert led["photons_terminated"] == 1000 and led["n_detected"] == 0
     t.close()
+
+
+def test_checkpoint_resume_bit_identical(tmp_path):
+    """A run stopped after its first portion and resumed from the checkpoint file gives the same
+    integer tallies and ledger as one uninterrupted run."""
+    from xmcml_b200 import checkpoint as CK
+    n = 60_000
+    xml, surf = scenes.planar(photons=n).write(str(tmp_path), "ck")
+    m = api.Model(xml, surf)
+    t = api.Transport(m, roulette=True)
+    t.run(n, seed=31)
+    whole = t.tallies()
+    whole_led = t.run(n, seed=31)
+    path = str(tmp_path / "run.ckpt")
+
+    class Stop(Exception):
+        pass
+
+    def stop(st):
+        if st.next_id >= 25_000:
+            raise Stop()
+
+    with pytest.raises(Stop):
+        CK.run_portions(t, CK.RunState(31, n, 25_000), path, stop)
+    st = CK.run_portions(t, CK.RunState.load(path), path)
+    assert st.done
+    for k, v in whole.items():
+        assert np.array_equal(st.tallies[k], v), k
+    for k in ("photons_launched", "steps", "absorbed_fx", "escaped_top_fx", "roulette_killed_fx", "roulette_gained_fx"):
+        assert st.ledger[k] == whole_led[k], k
+    t.close()

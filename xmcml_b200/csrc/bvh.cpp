@@ -360,23 +360,99 @@ int occupied_z_slabs(const GeomImage& g, float* lo, float* hi) {
 void build_xy_grid(const GeomImage& g, GridImage* out) {
     *out = GridImage();
     if (g.n_tris == 0) return;
-    float xlo = INFINITY, ylo = INFINITY, xhi = -INFINITY, yhi = -INFINITY;
-    for (int i = 0; i < g.n_tris; ++i)
+    struct Box { float ax, bx, ay, by, zl, zh; };
+    std::vector<Box> box(g.n_tris);
+    for (int t = 0; t < g.n_tris; ++t) {
+        Box& b = box[t];
+        b.ax = b.ay = b.zl = INFINITY;
+        b.bx = b.by = b.zh = -INFINITY;
         for (int c = 0; c < 3; ++c) {
-            const float4 v = g.tris[3 * (size_t)i + c];
-            xlo = std::min(xlo, v.x); xhi = std::max(xhi, v.x);
-            ylo = std::min(ylo, v.y); yhi = std::max(yhi, v.y);
+            const float4 v = g.tris[3 * (size_t)t + c];
+            b.ax = std::min(b.ax, v.x); b.bx = std::max(b.bx, v.x);
+            b.ay = std::min(b.ay, v.y); b.by = std::max(b.by, v.y);
+            b.zl = std::min(b.zl, v.z); b.zh = std::max(b.zh, v.z);
         }
-    const float padx = 1e-5f * std::max(1.0f, std::max(std::fabs(xlo), std::fabs(xhi)));
-    const float pady = 1e-5f * std::max(1.0f, std::max(std::fabs(ylo), std::fabs(yhi)));
-    xlo -= padx; xhi += padx; ylo -= pady; yhi += pady;
-    const double wx = std::max(1e-6f, xhi - xlo), wy = std::max(1e-6f, yhi - ylo);
-    // about two triangles per cell, square-ish cells, at most 1024 x 1024
-    const double cells = std::min(1048576.0, std::max(1.0, g.n_tris / 2.0));
-    int nx = (int)std::ceil(std::sqrt(cells * wx / wy));
-    nx = std::max(1, std::min(1024, nx));
-    int ny = (int)std::ceil(cells / nx);
-    ny = std::max(1, std::min(1024, ny));
+    }
+    // The grid covers the small triangles only: triangles spanning more than kBigTriangleCells cells
+    // (the planes of a layer stack) are tested by every query from a short list instead. Their
+    // extent must not set the grid's, so the bounds are refined a few times: grid over the current
+    // set, mark the big triangles, bounds of the rest.
+    std::vector<char> is_big(g.n_tris, 0);
+    float xlo = 0, ylo = 0, xhi = 0, yhi = 0, padx = 0, pady = 0;
+    int nx = 1, ny = 1;
+    double wx = 1, wy = 1;
+    for (int pass = 0; pass < 4; ++pass) {
+        xlo = ylo = INFINITY;
+        xhi = yhi = -INFINITY;
+        int n_small = 0;
+        for (int t = 0; t < g.n_tris; ++t) {
+            if (is_big[t]) continue;
+            ++n_small;
+            xlo = std::min(xlo, box[t].ax); xhi = std::max(xhi, box[t].bx);
+            ylo = std::min(ylo, box[t].ay); yhi = std::max(yhi, box[t].by);
+        }
+        if (n_small == 0) {  // every triangle is big: a one-cell grid with an empty cell
+            xlo = ylo = 0.0f;
+            xhi = yhi = 1.0f;
+        }
+        padx = 1e-5f * std::max(1.0f, std::max(std::fabs(xlo), std::fabs(xhi)));
+        pady = 1e-5f * std::max(1.0f, std::max(std::fabs(ylo), std::fabs(yhi)));
+        xlo -= padx; xhi += padx; ylo -= pady; yhi += pady;
+        wx = std::max(1e-6f, xhi - xlo);
+        wy = std::max(1e-6f, yhi - ylo);
+        // about two triangles per cell, square-ish cells, at most 1024 x 1024
+        const double cells = std::min(1048576.0, std::max(1.0, n_small / 2.0));
+        nx = (int)std::ceil(std::sqrt(cells * wx / wy));
+        nx = std::max(1, std::min(1024, nx));
+        ny = (int)std::ceil(cells / nx);
+        ny = std::max(1, std::min(1024, ny));
+        const double icx = nx / wx, icy = ny / wy;
+        std::vector<char> next(g.n_tris, 0);
+        int n_big = 0;
+        for (int t = 0; t < g.n_tris; ++t) {
+            // cells the triangle spans at this cell size (clamping ignored: a triangle outside the
+            // current bounds counts in full)
+            const double cx = std::floor((box[t].bx + padx - xlo) * icx) - std::floor((box[t].ax - padx - xlo) * icx) + 1;
+            const double cy = std::floor((box[t].by + pady - ylo) * icy) - std::floor((box[t].ay - pady - ylo) * icy) + 1;
+            if (is_big[t] || cx * cy > kBigTriangleCells) {
+                next[t] = 1;
+                ++n_big;
+            }
+        }
+        if (n_big > kMaxBigTriangles) {
+            // more large triangles than the list holds: no refinement, the grid covers every triangle
+            std::fill(is_big.begin(), is_big.end(), 0);
+            break;
+        }
+        if (next == is_big) break;
+        is_big.swap(next);
+    }
+    // final bounds and size from the final marking
+    {
+        xlo = ylo = INFINITY;
+        xhi = yhi = -INFINITY;
+        int n_small = 0;
+        for (int t = 0; t < g.n_tris; ++t) {
+            if (is_big[t]) continue;
+            ++n_small;
+            xlo = std::min(xlo, box[t].ax); xhi = std::max(xhi, box[t].bx);
+            ylo = std::min(ylo, box[t].ay); yhi = std::max(yhi, box[t].by);
+        }
+        if (n_small == 0) {
+            xlo = ylo = 0.0f;
+            xhi = yhi = 1.0f;
+        }
+        padx = 1e-5f * std::max(1.0f, std::max(std::fabs(xlo), std::fabs(xhi)));
+        pady = 1e-5f * std::max(1.0f, std::max(std::fabs(ylo), std::fabs(yhi)));
+        xlo -= padx; xhi += padx; ylo -= pady; yhi += pady;
+        wx = std::max(1e-6f, xhi - xlo);
+        wy = std::max(1e-6f, yhi - ylo);
+        const double cells = std::min(1048576.0, std::max(1.0, n_small / 2.0));
+        nx = (int)std::ceil(std::sqrt(cells * wx / wy));
+        nx = std::max(1, std::min(1024, nx));
+        ny = (int)std::ceil(cells / nx);
+        ny = std::max(1, std::min(1024, ny));
+    }
     out->nx = nx;
     out->ny = ny;
     out->x0 = xlo;
@@ -387,25 +463,27 @@ void build_xy_grid(const GeomImage& g, GridImage* out) {
     struct Span { int i0, i1, j0, j1; float zl, zh; };
     std::vector<Span> spans(g.n_tris);
     for (int t = 0; t < g.n_tris; ++t) {
-        float ax = INFINITY, bx = -INFINITY, ay = INFINITY, by = -INFINITY, zl = INFINITY, zh = -INFINITY;
-        for (int c = 0; c < 3; ++c) {
-            const float4 v = g.tris[3 * (size_t)t + c];
-            ax = std::min(ax, v.x); bx = std::max(bx, v.x);
-            ay = std::min(ay, v.y); by = std::max(by, v.y);
-            zl = std::min(zl, v.z); zh = std::max(zh, v.z);
-        }
-        const float pz = 1e-5f * std::max(1.0f, std::max(std::fabs(zl), std::fabs(zh)));
+        const Box& b = box[t];
+        const float pz = 1e-5f * std::max(1.0f, std::max(std::fabs(b.zl), std::fabs(b.zh)));
         Span& sp = spans[t];
-        sp.zl = zl - pz;
-        sp.zh = zh + pz;
-        sp.i0 = std::max(0, std::min(nx - 1, (int)std::floor((ax - padx - xlo) * out->icx)));
-        sp.i1 = std::max(0, std::min(nx - 1, (int)std::floor((bx + padx - xlo) * out->icx)));
-        sp.j0 = std::max(0, std::min(ny - 1, (int)std::floor((ay - pady - ylo) * out->icy)));
-        sp.j1 = std::max(0, std::min(ny - 1, (int)std::floor((by + pady - ylo) * out->icy)));
+        sp.zl = b.zl - pz;
+        sp.zh = b.zh + pz;
+        sp.i0 = std::max(0, std::min(nx - 1, (int)std::floor((b.ax - padx - xlo) * out->icx)));
+        sp.i1 = std::max(0, std::min(nx - 1, (int)std::floor((b.bx + padx - xlo) * out->icx)));
+        sp.j0 = std::max(0, std::min(ny - 1, (int)std::floor((b.ay - pady - ylo) * out->icy)));
+        sp.j1 = std::max(0, std::min(ny - 1, (int)std::floor((b.by + pady - ylo) * out->icy)));
     }
     auto as_float = [](int t) { float f; std::memcpy(&f, &t, sizeof(f)); return f; };
-    std::vector<char> is_big(g.n_tris, 0);
+    // the big list: every triangle marked above (at most kMaxBigTriangles; they may lie outside the
+    // grid's bounds), then, while there is room, triangles that span too many cells of the final grid
+    for (int t = 0; t < g.n_tris; ++t) {
+        if (!is_big[t]) continue;
+        const Span& sp = spans[t];
+        out->big.push_back(make_float4(sp.zl, sp.zh, as_float(t), 0.0f));
+        for (int c = 0; c < 3; ++c) out->big.push_back(g.tris[3 * (size_t)t + c]);
+    }
     for (int t = 0; t < g.n_tris && (int)(out->big.size() / 4) < kMaxBigTriangles; ++t) {
+        if (is_big[t]) continue;
         const Span& sp = spans[t];
         const long long covered = (long long)(sp.i1 - sp.i0 + 1) * (sp.j1 - sp.j0 + 1);
         if (covered > kBigTriangleCells) {

@@ -165,11 +165,12 @@ __host__ __device__ __forceinline__ bool grid_nearest(const uint2* __restrict__ 
     const float fy1 = fminf(fmaxf((fmaxf(oy, ey) - gy0) * icy, -1.0f), (float)ny);
     h.t = tmax;
     h.tri = -1;
-    if (!(fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)nx && fy0 < (float)ny)) return true;  // outside every triangle
+    const bool inside = fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)nx && fy0 < (float)ny;
     const int i0 = max(0, (int)floorf(fx0)), i1 = min(nx - 1, (int)floorf(fx1));
     const int j0 = max(0, (int)floorf(fy0)), j1 = min(ny - 1, (int)floorf(fy1));
-    if ((i1 - i0 + 1) * (j1 - j0 + 1) > kGridMaxCells) return false;
+    if (inside && (i1 - i0 + 1) * (j1 - j0 + 1) > kGridMaxCells) return false;
     const float zl = fminf(oz, ez), zh = fmaxf(oz, ez);
+    // the large triangles (they may extend beyond the grid's bounds), then the cells
     for (int k = 0; k < n_big; ++k) {
         const float4 en = big[4 * k];
         if (en.y < zl || en.x > zh) continue;
@@ -178,6 +179,7 @@ __host__ __device__ __forceinline__ bool grid_nearest(const uint2* __restrict__ 
         ++n_tri;
         grid_candidate(big[4 * k + 1], big[4 * k + 2], big[4 * k + 3], t, ox, oy, oz, dx, dy, dz, tmin, retests, h);
     }
+    if (!inside) return true;  // every other triangle lies inside the grid's bounds
     for (int j = j0; j <= j1; ++j) {
         for (int i = i0; i <= i1; ++i) {
             const unsigned int ci = (unsigned int)j * (unsigned int)nx + (unsigned int)i;

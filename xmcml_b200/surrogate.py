@@ -133,3 +133,135 @@ def to_bf16_bits(x: np.ndarray) -> np.ndarray:
 
 def from_bf16_bits(b: np.ndarray) -> np.ndarray:
     return (np.asarray(b, dtype=np.uint32) << 16).view(np.float32)
+
+
+# ---------------------------------------------------------------------------------------------
+# Surrogate of the batched Monte Carlo
+
+def reflectance_targets(ring_time: np.ndarray, floor: float = 1e-8) -> np.ndarray:
+    """Network targets from MC tallies: log10 of the ring x time reflectance (fraction of launched
+    weight per cell) with a floor below the MC's resolution; [n, rings * time]."""
+    r = np.asarray(ring_time, dtype=np.float64).reshape(len(ring_time), -1)
+    return np.log10(np.maximum(r, 0.0) + floor)
+
+
+def relative_error(pred_log: np.ndarray, ref: np.ndarray, ref_w2: np.ndarray, photons: np.ndarray,
+                   floor: float = 1e-8, max_ref_rse: float = 0.01) -> np.ndarray:
+    """Per-cell |R_pred / R_ref - 1| on the cells whose reference is known to max_ref_rse (relative
+    standard error from the tally of squared weights); other cells are NaN."""
+    ref = np.asarray(ref, dtype=np.float64).reshape(len(ref), -1)
+    w2 = np.asarray(ref_w2, dtype=np.float64).reshape(len(ref), -1)
+    n = np.asarray(photons, dtype=np.float64)[:, None]
+    # per-photon variance of the cell's score: E[w^2] - E[w]^2 (fractions of launched weight)
+    var = np.maximum(w2 / n - ref * ref, 0.0) / n
+    rse = np.sqrt(var) / np.maximum(ref, 1e-300)
+    pred = 10.0 ** np.asarray(pred_log, dtype=np.float64) - floor
+    err = np.abs(pred / np.maximum(ref, 1e-300) - 1.0)
+    err[(ref <= 0) | (rse > max_ref_rse)] = np.nan
+    return err
+
+
+def he_uniform(rng: np.random.Generator, n_in: int, hidden: int, n_hidden: int, n_out: int) -> np.ndarray:
+    """Initial parameters in the flat layout: He-uniform weights, zero biases."""
+    dims = [n_in] + [hidden] * n_hidden + [n_out]
+    parts = []
+    for i in range(len(dims) - 1):
+        lim = np.sqrt(6.0 / dims[i])
+        parts += [rng.uniform(-lim, lim, dims[i + 1] * dims[i]), np.zeros(dims[i + 1])]
+    return np.concatenate(parts).astype(np.float32)
+
+
+class Surrogate:
+    """Ensemble of MLPs over standardised features and targets, with the training hull and an
+    ensemble-spread gate; `reflectance` falls back to the batched Monte Carlo where either check
+    fails."""
+
+    def __init__(self, n_in: int = 15, n_out: int = 1000, members: int = 4, hidden: int = 256, n_hidden: int = 4,
+                 max_rows: int = 65536, device: int = 0, floor: float = 1e-8, gate: float = 0.02,
+                 hull_margin: float = 0.0):
+        self.members = [MLP(n_in, n_out, hidden, n_hidden, max_rows, device) for _ in range(members)]
+        self.n_in, self.n_out, self.floor, self.gate, self.hull_margin = n_in, n_out, floor, gate, hull_margin
+        self.hidden, self.n_hidden = hidden, n_hidden
+        self.x_mean = np.zeros(n_in); self.x_std = np.ones(n_in)
+        self.y_mean = np.zeros(n_out); self.y_std = np.ones(n_out)
+        self.lo = np.full(n_in, -np.inf); self.hi = np.full(n_in, np.inf)
+        self.train_ms = 0.0
+
+    # ---- training ----
+    def fit(self, features: np.ndarray, targets: np.ndarray, steps: int = 4000, batch: int = 4096, lr: float = 2e-3,
+            seed: int = 1, phases: int = 4) -> List[np.ndarray]:
+        """Standardise, then train every member from its own initialisation and minibatch stream
+        with Adam; the learning rate drops by 3x at each of `phases` equal phases. Returns the
+        loss curves (standardised units)."""
+        f = np.asarray(features, dtype=np.float64)
+        y = np.asarray(targets, dtype=np.float64)
+        self.x_mean, self.x_std = f.mean(0), f.std(0) + 1e-12
+        self.y_mean, self.y_std = y.mean(0), y.std(0) + 1e-6
+        self.lo, self.hi = f.min(0), f.max(0)
+        xs = ((f - self.x_mean) / self.x_std).astype(np.float32)
+        ys = ((y - self.y_mean) / self.y_std).astype(np.float32)
+        curves = []
+        self.train_ms = 0.0
+        for i, m in enumerate(self.members):
+            rng = np.random.default_rng(seed * 1000 + i)
+            m.set_params(he_uniform(rng, self.n_in, self.hidden, self.n_hidden, self.n_out))
+            m.set_dataset(xs, ys)
+            curve = []
+            per = max(1, steps // phases)
+            done = 0
+            for ph in range(phases):
+                n = per if ph < phases - 1 else steps - done
+                if n <= 0:
+                    break
+                losses, ms = m.train(n, batch=batch, lr=lr / 3 ** ph, seed=seed * 7919 + i)
+                curve.append(losses)
+                self.train_ms += ms
+                done += n
+            curves.append(np.concatenate(curve) if curve else np.zeros(0))
+        return curves
+
+    # ---- inference ----
+    def in_hull(self, features: np.ndarray) -> np.ndarray:
+        f = np.asarray(features, dtype=np.float64)
+        span = self.hi - self.lo
+        return np.all((f >= self.lo - self.hull_margin * span) & (f <= self.hi + self.hull_margin * span), axis=1)
+
+    def predict(self, features: np.ndarray) -> Dict[str, np.ndarray]:
+        """mean / spread of log10 reflectance over the ensemble, and the gate: in the training hull
+        and median ensemble spread (in relative reflectance, ln 10 x std of log10) below `gate`."""
+        f = np.asarray(features, dtype=np.float64)
+        xs = ((f - self.x_mean) / self.x_std).astype(np.float32)
+        outs, ms = [], 0.0
+        for m in self.members:
+            y, t = m.forward(xs)
+            outs.append(y.astype(np.float64) * self.y_std + self.y_mean)
+            ms += t
+        stack = np.stack(outs)
+        mean = stack.mean(0)
+        spread = stack.std(0) * np.log(10.0) if len(outs) > 1 else np.zeros_like(mean)
+        # the spread that matters is where the reflectance is above the floor
+        sig = mean > np.log10(self.floor) + 1.0
+        med = np.array([np.median(s[g]) if g.any() else 0.0 for s, g in zip(spread, sig)])
+        ok = self.in_hull(f) & (med <= self.gate)
+        return {"log10_r": mean, "spread": med, "use_network": ok, "ms": ms}
+
+    def reflectance(self, inst, batch=None, fallback_photons: int = 10 ** 6) -> Dict[str, np.ndarray]:
+        """Ring x time reflectance [n, n_out] of the instances: from the network where the gate
+        allows it, else from the batched Monte Carlo with `fallback_photons` photons each."""
+        p = self.predict(inst.features())
+        r = 10.0 ** p["log10_r"] - self.floor
+        fb = np.nonzero(~p["use_network"])[0]
+        if fb.size:
+            from .batch import Batch
+            own = batch is None
+            b = batch or Batch(n_layers=inst.n_layers, max_instances=max(int(fb.size), 1))
+            sub = inst.subset(fb).with_photons(fallback_photons)
+            out = b.run(sub)
+            r[fb] = out["ring_time"].reshape(len(fb), -1)
+            if own:
+                b.close()
+        return {"reflectance": r, "from_network": p["use_network"], "spread": p["spread"]}
+
+    def close(self):
+        for m in self.members:
+            m.close()

@@ -44,7 +44,9 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["heightfield", "planar", "ellipsoid"], default="heightfield")
+    p.add_argument("--workload", choices=["heightfield", "planar", "ellipsoid", "batch"], default="heightfield")
+    p.add_argument("--instances", type=int, default=1024)
+    p.add_argument("--budget-scale", type=float, default=1.0)
     p.add_argument("--photons", type=int, default=10_000_000)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -151,7 +153,17 @@ def run_reference_arm(args, rank, world):
         return
     os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
     d = tempfile.mkdtemp(prefix="xmc_bench_ref_")
-    sc, cfg = make_scene(args.workload, args.photons)
+    inst = None
+    if args.workload == "batch":
+        # the instances one after the other through the reference's LaunchOMP (the reference has no
+        # batched form): a bounded sample of photons from instance k at step k
+        from xmcml_b200 import batch as XB
+        inst = XB.sample_instances(2024, args.instances, budget=(1e5 * args.budget_scale, 1e7 * args.budget_scale))
+        sc = XB.to_scene(inst, 0)
+        cfg = {"workload": f"batched-{args.instances}-instances-3layer", "rings": 50, "time_bins": "20 x 50 ps",
+               "sample": "instance k at step k"}
+    else:
+        sc, cfg = make_scene(args.workload, args.photons)
     xml, surf = sc.write(d, "bench")
     from oracle import bind as OB
     if not OB.ref_available(fast=True):
@@ -168,6 +180,10 @@ def run_reference_arm(args, rank, world):
     OB.ref(True).ref_free_output(C.byref(out))
     times = []
     for k in range(args.steps):
+        if inst is not None and k > 0:  # the sweep's next instance, same sample size
+            xml, surf = XB.to_scene(inst, k % len(inst)).write(d, f"bench{k}")
+            info = OB.ref_load_model(xml, surf, fast=True)
+            OB.ref(True).ref_generate_bvh(C.byref(info))
         out = OB.ref_new_output(info, fast=True)
         t0 = time.perf_counter()
         OB.ref_launch(info, out, 777 + k, threads, fast=True, n=n_step)
@@ -178,7 +194,8 @@ def run_reference_arm(args, rank, world):
     cfg = dict(cfg)
     cfg["parallelism"] = f"OpenMP x{threads} (host CPU)"
     cfg["semantics"] = "reference: weight cut at MinWeight 1e-4, Area kill (no roulette in the reference)"
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+    metric = "photons/s (batched 3-layer instances)" if inst is not None else METRIC
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
@@ -289,6 +306,81 @@ def surrogate_inference(local):
             "error_note": "accuracy of the trained ensemble is measured by xmcml_b200.surrogate_study, not here"}
 
 
+def run_batch_workload(args, rank, world, local, dist, torch, barrier):
+    """Batched sweep: `instances` 3-layer planar instances (the sweep's distributions, photon budgets
+    log-uniform in [1e5, 1e7] x budget_scale) in one persistent launch per step, replayed from a
+    CUDA graph, launch shape from the autotuner. value: photons / device time of the transport
+    kernel; e2e: photons / host wall time of xmc_batch_run (instance table upload, zeroing, kernel,
+    FP64 reduction and read-back of [instances x 50 x 20] reflectance and the ledgers)."""
+    import numpy as np
+    from xmcml_b200 import batch as XB
+    from xmcml_b200 import replicas
+    K = args.instances
+    inst = XB.sample_instances(2024 + rank, K, budget=(1e5 * args.budget_scale, 1e7 * args.budget_scale))
+    total = int(inst.photons.sum())
+    b = XB.Batch(max_instances=K, device=local)
+    tune = b.autotune(inst.subset(np.arange(min(128, K))), photons_cap=20000)
+    for w in range(args.warmup):
+        b.run(inst)
+    barrier()
+    kms, walls, steps = [], [], 0
+    with ClockSampler(local) as clk:
+        barrier()
+        for k in range(args.steps):
+            t0 = time.perf_counter()
+            out = b.run(inst)
+            walls.append(time.perf_counter() - t0)
+            kms.append(out["kernel_ms"])
+            steps = int(out["steps"].sum())
+        barrier()
+    clocks = clk.summary()
+    dev = torch.device(f"cuda:{local}")
+    ker_ms = replicas.max_over_ranks(sum(kms), dist, dev)
+    wall_s = replicas.max_over_ranks(sum(walls), dist, dev)
+    value = world * args.steps * total / (ker_ms / 1e3)
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    t = ker_ms / args.steps / 1e3
+    ops = steps * (48 + 45)
+    peak = 148 * 128 * sm_mhz * 1e6
+    rl = {"bound": "issue", "achieved": ops / t / 1e12, "peak": peak / 1e12, "unit": "TOP/s", "frac": ops / t / peak,
+          "traffic": None, "model": {"ops_per_step": 93, "steps_per_photon": steps / total,
+                                     "peak_source": "nominal 148 SMs x 128 lanes x median sampled SM clock"}}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import bind as OB
+            if OB.ref_available(fast=True):
+                d = tempfile.mkdtemp(prefix="xmc_bench_batch_")
+                rates = []
+                for k in range(4):
+                    xml, surf = XB.to_scene(inst, k).write(d, f"i{k}")
+                    r, n_cpu, secs = cpu_reference_rate(xml, surf, args.cpu_seconds / 4, os.cpu_count() or 1)
+                    rates.append(r)
+                cpu = {"value": float(np.mean(rates)), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference",
+                       "sample": "the reference's LaunchOMP on the first 4 instances as planar models, "
+                                 f"{args.cpu_seconds / 4:.0f} s each, mean rate (weight cut semantics)"}
+        except Exception as e:
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference", "sample": f"failed: {e}"}
+    b.close()
+    R, T = 50, 20
+    line = {"metric": "photons/s (batched 3-layer instances)", "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ker_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched-{K}-instances-3layer", "photons_per_step": total,
+                       "budgets": f"log-uniform [{1e5 * args.budget_scale:.0e}, {1e7 * args.budget_scale:.0e}]",
+                       "rings": R, "time_bins": f"{T} x 50 ps", "roulette": "1e-4 / 0.1", "autotune": tune,
+                       "parallelism": f"replicas x{world} (disjoint instance sets)",
+                       "l2": "instance table re-uploaded and 24.6 MB of tallies zeroed every step"},
+            "clocks": clocks,
+            "e2e": {"value": world * args.steps * total / wall_s, "unit": UNIT,
+                    "h2d_bytes_per_step": K * (32 + 5 * 48), "d2h_bytes_per_step": K * (R * T * 8 + R * 8 + 16 * 8) + 4,
+                    "via": "xmc_batch_run with host instance table and host result arrays"},
+            "gpu_launches": 2 * args.steps, "roofline": rl, "cpu_baseline": cpu,
+            "walk": {"steps_per_photon": steps / total}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -310,6 +402,13 @@ def main():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
+
+    if args.workload == "batch":
+        run_batch_workload(args, rank, world, local, dist, torch, barrier)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     from xmcml_b200 import api, _lib
     from xmcml_b200 import structs as S

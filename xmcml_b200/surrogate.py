@@ -178,9 +178,10 @@ class Surrogate:
 
     def __init__(self, n_in: int = 15, n_out: int = 1000, members: int = 4, hidden: int = 256, n_hidden: int = 4,
                  max_rows: int = 65536, device: int = 0, floor: float = 1e-8, gate: float = 0.02,
-                 hull_margin: float = 0.0):
+                 hull_margin: float = 0.0, gate_floor: float = 1e-5):
         self.members = [MLP(n_in, n_out, hidden, n_hidden, max_rows, device) for _ in range(members)]
         self.n_in, self.n_out, self.floor, self.gate, self.hull_margin = n_in, n_out, floor, gate, hull_margin
+        self.gate_floor = gate_floor
         self.hidden, self.n_hidden = hidden, n_hidden
         self.x_mean = np.zeros(n_in); self.x_std = np.ones(n_in)
         self.y_mean = np.zeros(n_out); self.y_std = np.ones(n_out)
@@ -239,8 +240,8 @@ class Surrogate:
         stack = np.stack(outs)
         mean = stack.mean(0)
         spread = stack.std(0) * np.log(10.0) if len(outs) > 1 else np.zeros_like(mean)
-        # the spread that matters is where the reflectance is above the floor
-        sig = mean > np.log10(self.floor) + 1.0
+        # the spread that matters is where the reflectance is well above the Monte Carlo's resolution
+        sig = mean > np.log10(max(self.gate_floor, self.floor))
         med = np.array([np.median(s[g]) if g.any() else 0.0 for s, g in zip(spread, sig)])
         ok = self.in_hull(f) & (med <= self.gate)
         return {"log10_r": mean, "spread": med, "use_network": ok, "ms": ms}

@@ -523,6 +523,9 @@ int xmc_mlp_set_dataset(xmc_mlp* m, const float* x, const float* t, int rows);
  * (Philox keyed by seed); losses[steps] (may be NULL) = each minibatch's mean squared error. */
 int xmc_mlp_train(xmc_mlp* m, int steps, int batch, float lr, float beta1, float beta2, float eps,
                   uint64_t seed, float* losses, double* ms);
+/* Per-output weights w[n_out] >= 0 of the squared error in training and xmc_mlp_gradients
+ * (loss = mean over rows and outputs of w_j (y_j - t_j)^2); NULL restores all weights to 1. */
+int xmc_mlp_set_output_weights(xmc_mlp* m, const float* w);
 int xmc_mlp_destroy(xmc_mlp* m);
 
 /* D[M][N] = A[M][K] . B[N][K]^T on the tensor cores (bf16 inputs as raw 16-bit patterns, FP32

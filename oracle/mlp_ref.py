@@ -77,15 +77,17 @@ def forward(p, x, n_in, hidden, n_hidden, n_out, emulate=True, keep=False):
     return (Y, acts, pre) if keep else Y
 
 
-def gradients(p, x, t, n_in, hidden, n_hidden, n_out, emulate=True):
-    """(flat gradient of the mean squared error, loss)."""
+def gradients(p, x, t, n_in, hidden, n_hidden, n_out, emulate=True, w=None):
+    """(flat gradient of the mean squared error, loss); w: optional per-output weights of the
+    squared error."""
     q = bf16 if emulate else (lambda v: np.asarray(v, dtype=np.float64))
     layers = unflatten(np.asarray(p, dtype=np.float32), n_in, hidden, n_hidden, n_out)
     Y, acts, pre = forward(p, x, n_in, hidden, n_hidden, n_out, emulate, keep=True)
     rows = x.shape[0]
     D = Y - t
-    loss = float(np.mean(D * D))
-    dZ = q(D * (2.0 / (rows * n_out)))
+    wv = np.ones(n_out) if w is None else np.asarray(w, dtype=np.float64)
+    loss = float(np.mean(wv * D * D))
+    dZ = q(wv * D * (2.0 / (rows * n_out)))
     grads = [None] * len(layers)
     for i in range(len(layers) - 1, -1, -1):
         W, _ = layers[i]

@@ -59,12 +59,15 @@ def test_forward_matches_oracle():
     m.close()
 
 
-def test_gradients_match_oracle():
+@pytest.mark.parametrize("weighted", [False, True])
+def test_gradients_match_oracle(weighted):
     m, p, rng = _model_and_params(2)
     x = rng.standard_normal((512, 15)).astype(np.float32)
     t = (R.forward(p, x, **DIMS) + rng.normal(0, 0.5, (512, 1000))).astype(np.float32)
+    w = rng.uniform(0.05, 2.0, 1000).astype(np.float32) if weighted else None
+    m.set_output_weights(w)
     g, loss = m.gradients(x, t)
-    gr, lr_ = R.gradients(p, x, t, **DIMS)
+    gr, lr_ = R.gradients(p, x, t, **DIMS, w=w)
     assert loss == pytest.approx(lr_, rel=1e-3)
     o = 0
     for i, (r, c) in enumerate(R.shapes(15, 256, 4, 1000)):

@@ -115,8 +115,8 @@ struct EpiHidden {
 };
 
 // Output layer: Y = acc + b for the first n_out columns. Training (t != nullptr): the gradient of
-// the mean squared error dY = scale (Y - T) (0 in the padding columns), row-major and transposed,
-// and the sum of squared errors added to loss[*step].
+// the (optionally per-output weighted) mean squared error dY = scale w (Y - T) (0 in the padding
+// columns), row-major and transposed, and the sum of w (Y - T)^2 added to loss[*step].
 struct EpiOut {
     const float* bias;
     float* y;  // nullable, [rows x ldy]
@@ -129,6 +129,7 @@ struct EpiOut {
     bf16* dyt;
     int lddyt;
     float scale;
+    const float* colw;  // nullable: per-output weight of the squared error
     float* loss;
     const int* step;
     __device__ void apply(int row, int col0, const uint32_t (&r)[32], int lane) const {
@@ -151,8 +152,9 @@ struct EpiOut {
             for (int j = 0; j < 32; ++j) {
                 const int c = col0 + j;
                 const float d = c < n_out ? v[j] - __ldg(&tp[c]) : 0.0f;
-                se = fmaf(d, d, se);
-                v[j] = d * scale;
+                const float wd = (colw && c < n_out) ? d * __ldg(&colw[c]) : d;
+                se = fmaf(wd, d, se);
+                v[j] = wd * scale;
             }
             store_bf16x32(dy + (size_t)row * lddy + col0, v);
 #pragma unroll
@@ -389,6 +391,7 @@ struct xmc_mlp {
     bf16 *a[kMaxLayers] = {}, *at[kMaxLayers] = {}, *z[kMaxLayers] = {};
     bf16 *dz[kMaxLayers] = {}, *dzt[kMaxLayers] = {};
     float *y = nullptr, *t = nullptr, *xin = nullptr;
+    float* colw = nullptr;          // per-output loss weights, or null
     float* part = nullptr;
     size_t part_floats = 0;
     // data set
@@ -409,7 +412,8 @@ void free_mlp(xmc_mlp* m) {
     cudaSetDevice(m->spec.device);
     for (auto& kv : m->train_graphs) cudaGraphExecDestroy(kv.second);
     for (auto& kv : m->fwd_graphs) cudaGraphExecDestroy(kv.second);
-    std::vector<void*> d = {m->d_err, m->d_step, m->d_loss, m->x, m->xt, m->y, m->t, m->xin, m->part, m->ds_x, m->ds_t};
+    std::vector<void*> d = {m->d_err, m->d_step, m->d_loss, m->x, m->xt, m->y, m->t, m->xin, m->part, m->ds_x, m->ds_t,
+                            m->colw};
     for (int l = 0; l < kMaxLayers; ++l)
         for (void* p : {(void*)m->w32[l], (void*)m->b32[l], (void*)m->mw[l], (void*)m->vw[l], (void*)m->mb[l],
                         (void*)m->vb[l], (void*)m->gw[l], (void*)m->gb[l], (void*)m->w16[l], (void*)m->w16t[l],
@@ -456,6 +460,7 @@ int enqueue_forward(xmc_mlp* m, int rows, bool train) {
                 e.dyt = m->dzt[l];
                 e.lddyt = rows;
                 e.scale = 2.0f / ((float)rows * (float)m->spec.n_out);
+                e.colw = m->colw;
                 e.loss = m->d_loss;
                 e.step = m->d_step;
             } else {
@@ -846,6 +851,26 @@ extern "C" int xmc_mlp_train(xmc_mlp* m, int steps, int batch, float lr, float b
         const float inv = 1.0f / ((float)batch * (float)m->spec.n_out);
         for (int i = 0; i < steps; ++i) losses[i] *= inv;
     }
+    return XMC_OK;
+}
+
+// Per-output weights of the squared error in training and in xmc_mlp_gradients (NULL: all 1).
+extern "C" int xmc_mlp_set_output_weights(xmc_mlp* m, const float* w) {
+    if (!m) return mfail(XMC_ERR_INVALID_INPUT, "model is NULL");
+    XM_CUDA(cudaSetDevice(m->spec.device));
+    XM_CUDA(cudaStreamSynchronize(m->stream));
+    if (!w) {
+        if (m->colw) cudaFree(m->colw);
+        m->colw = nullptr;
+    } else {
+        for (int j = 0; j < m->spec.n_out; ++j)
+            if (!(w[j] >= 0.0f) || !std::isfinite(w[j])) return mfail(XMC_ERR_INVALID_INPUT, "weights must be finite and >= 0");
+        if (!m->colw) XM_CUDA(cudaMalloc(&m->colw, sizeof(float) * m->spec.n_out));
+        XM_CUDA(cudaMemcpy(m->colw, w, sizeof(float) * m->spec.n_out, cudaMemcpyHostToDevice));
+    }
+    // the training graphs hold the old pointer
+    for (auto& kv : m->train_graphs) cudaGraphExecDestroy(kv.second);
+    m->train_graphs.clear();
     return XMC_OK;
 }
 

@@ -4,7 +4,7 @@
 //
 // One CTA of 128 threads computes a 128 x BN tile of D over a range of K (split-K when the grid's
 // z extent is > 1). Operand tiles of 128 (A) and BN (B) rows x 64 bf16 (128 B) are brought into
-// shared memory by TMA (cp.async.bulk.tensor.2d, 128-byte swizzle) through a 4-stage ring of
+// shared memory by TMA (cp.async.bulk.tensor.2d, 128-byte swizzle) through a 2-stage ring of
 // mbarrier-tracked buffers; one thread issues the tcgen05.mma instructions (M = 128, N = BN,
 // K = 16 each, both operands K-major, read from shared memory through matrix descriptors) into a
 // TMEM accumulator of BN columns, and tcgen05.commit signals the ring's "empty" barriers and the
@@ -24,7 +24,8 @@ namespace tc {
 
 constexpr int kBM = 128;          // tile rows (MMA M)
 constexpr int kBK = 64;           // K per stage: 64 bf16 = one 128-byte swizzle row
-constexpr int kStages = 4;
+constexpr int kStages = 2;  // small enough that two CTAs (BN = 256) share an SM: one's epilogue
+                              // overlaps the other's loads and MMAs
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of any single pipeline wait: 2 s
 
 __host__ __device__ constexpr int stage_bytes(int bn) { return (kBM + bn) * kBK * 2; }

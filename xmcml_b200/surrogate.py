@@ -57,6 +57,17 @@ class MLP:
         check(self._lib.xmc_mlp_get_params(self._m, p.ctypes.data_as(FP)))
         return p
 
+    def set_output_weights(self, w: Optional[np.ndarray]) -> None:
+        """Per-output weights of the squared error (None: all 1)."""
+        if w is None:
+            check(self._lib.xmc_mlp_set_output_weights(self._m, None))
+        else:
+            w = _f32(w)
+            if w.size != self.n_out:
+                raise ValueError("need one weight per output")
+            self._w = w
+            check(self._lib.xmc_mlp_set_output_weights(self._m, w.ctypes.data_as(FP)))
+
     def forward(self, x: np.ndarray) -> Tuple[np.ndarray, float]:
         """(outputs [n, n_out] float32, device ms); rows padded to a multiple of 128 internally."""
         x = _f32(x)
@@ -190,10 +201,12 @@ class Surrogate:
 
     # ---- training ----
     def fit(self, features: np.ndarray, targets: np.ndarray, steps: int = 4000, batch: int = 4096, lr: float = 2e-3,
-            seed: int = 1, phases: int = 4) -> List[np.ndarray]:
+            seed: int = 1, phases: int = 4, weighted: bool = False) -> List[np.ndarray]:
         """Standardise, then train every member from its own initialisation and minibatch stream
-        with Adam; the learning rate drops by 3x at each of `phases` equal phases. Returns the
-        loss curves (standardised units)."""
+        with Adam; the learning rate drops by 3x at each of `phases` equal phases. With `weighted`,
+        each output's squared error is weighted by the share of training rows in which it is above
+        gate_floor (at least 0.05; mean 1), so that outputs the Monte Carlo rarely resolves do not
+        dominate the fit. Returns the loss curves (standardised units)."""
         f = np.asarray(features, dtype=np.float64)
         y = np.asarray(targets, dtype=np.float64)
         self.x_mean, self.x_std = f.mean(0), f.std(0) + 1e-12
@@ -201,11 +214,17 @@ class Surrogate:
         self.lo, self.hi = f.min(0), f.max(0)
         xs = ((f - self.x_mean) / self.x_std).astype(np.float32)
         ys = ((y - self.y_mean) / self.y_std).astype(np.float32)
+        w = None
+        if weighted:
+            share = np.mean(y > np.log10(max(self.gate_floor, self.floor)), axis=0)
+            w = np.maximum(share, 0.05)
+            w = w / w.mean()
         curves = []
         self.train_ms = 0.0
         for i, m in enumerate(self.members):
             rng = np.random.default_rng(seed * 1000 + i)
             m.set_params(he_uniform(rng, self.n_in, self.hidden, self.n_hidden, self.n_out))
+            m.set_output_weights(w)
             m.set_dataset(xs, ys)
             curve = []
             per = max(1, steps // phases)

@@ -51,6 +51,7 @@ def main(argv=None):
     p.add_argument("--gate", type=float, default=0.05)
     p.add_argument("--seed", type=int, default=2024)
     p.add_argument("--device", type=int, default=0)
+    p.add_argument("--weighted", action="store_true")
     p.add_argument("--out", default="")
     a = p.parse_args(argv)
 
@@ -70,7 +71,7 @@ def main(argv=None):
                        gate=a.gate)
     t0 = time.perf_counter()
     curves = sur.fit(train.features(), SG.reflectance_targets(rt_tr, a.floor), steps=a.steps, batch=a.batch, lr=a.lr,
-                     seed=a.seed)
+                     seed=a.seed, weighted=a.weighted)
     t_fit = time.perf_counter() - t0
     pred = sur.predict(test.features())
     err = SG.relative_error(pred["log10_r"], rt_te, w2_te, test.photons, floor=a.floor, max_ref_rse=0.01)
@@ -88,7 +89,7 @@ def main(argv=None):
     evals = 65536 / (ms_fwd / 1e3) / a.members
     mc_rate = float(test.photons.sum()) / (ms_te / 1e3)
     res = {
-        "train_instances": a.train, "train_photons": a.train_photons, "test_instances": a.test,
+        "weighted_loss": a.weighted, "floor": a.floor, "train_instances": a.train, "train_photons": a.train_photons, "test_instances": a.test,
         "test_photons": a.test_photons, "members": a.members, "steps": a.steps, "batch": a.batch,
         "autotune": tune,
         "mc_train_photons_per_s": float(train.photons.sum()) / (ms_tr / 1e3), "mc_train_wall_s": t_gen,

@@ -256,6 +256,9 @@ typedef struct xmc_ledger {
     uint64_t absorbed_target_fx;   /* weight dropped while in a layer flagged in targetRangeLayers
                                     * (inside or outside Area; a part of absorbed + absorbed_outside) */
     double absorbed_target;        /* the same per launched photon                               */
+    uint64_t bias_gained_fx;       /* biasing: weight added by the weight-table factor W / p > 1  */
+    uint64_t bias_lost_fx;         /* biasing: weight removed by factors < 1                      */
+    double bias_gained, bias_lost; /* the same per launched photon                               */
 } xmc_ledger;
 
 typedef struct xmc_context xmc_context;
@@ -362,6 +365,14 @@ bool xmc_write_output_file(InputInfo* input, OutputInfo* output, const char* fil
 BVHTree* xmc_generate_bvh_tree(const Surface* surfaces, int numberOfSurfaces);
 void xmc_free_bvh_tree(BVHTree* tree);
 
+/* Replaces the computing branch of GetWeightIntegralTable (base/xmcml/xmcmlLauncher/weight_integral.cpp:
+ * 17-104, mcml_integration.cpp:7-83): the biased walk's weight-integral tables, one per distinct
+ * anisotropy of layers 1..numberOfLayers-1, weightTablePrecision + 1 values each, computed on GPU
+ * `device` in FP64 and stored in input->weightTable / numberOfWeightTables (new[]-allocated; freed
+ * by xmc_free_input; a previous table is not freed). xmc_create computes them itself when
+ * input->useBiasing is set and input->weightTable is NULL. */
+int xmc_weight_integral_table(InputInfo* input, int device);
+
 /* Replaces ComputeSpecularReflectance (base/xmcml/xmcml/mcml_kernel.cpp:16-37). */
 double xmc_specular_reflectance(const LayerInfo* layer);
 
@@ -429,7 +440,7 @@ typedef struct xmc_batch_instance {
 
 /* Launch shape of the batched kernel; chosen by xmc_batch_autotune or set by the caller. */
 typedef struct xmc_batch_tuning {
-    int32_t block_size;         /* threads per block, multiple of 32, <= 512                   */
+    int32_t block_size;         /* threads per block, multiple of 32, <= 256                   */
     int32_t blocks_per_sm;      /* resident blocks per SM (0 = as many as fit)                 */
     int32_t photons_per_chunk;  /* photon ids a warp takes from the dispenser at a time        */
     int32_t tally_scheme;       /* 0: per-photon global atomics for the instance ledger;
@@ -475,7 +486,8 @@ int xmc_batch_set_tuning(xmc_batch* b, const xmc_batch_tuning* t);
 int xmc_batch_get_tuning(const xmc_batch* b, xmc_batch_tuning* t);
 
 /* Times the batched kernel on `sample` (n instances, each capped at photons_cap photons) for
- * every candidate launch shape (block size x blocks per SM x photons per chunk x tally scheme),
+ * every candidate launch shape (block size {64, 128, 256} x photons per chunk {32, 64, 128, 256} x
+ * tally scheme {0, 1}, as many blocks per SM as fit),
  * keeps the fastest in `b` and returns it in *best. */
 int xmc_batch_autotune(xmc_batch* b, const xmc_batch_instance* sample, int n, uint64_t photons_cap,
                        xmc_batch_tuning* best);

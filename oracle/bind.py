@@ -38,7 +38,8 @@ _TERMS = ["specular", "absorbed", "absorbed_outside", "escaped_top", "escaped_bo
 
 
 class OracleLedger(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in _CNT] + [(n, C.c_double) for n in _TERMS] + [("absorbed_target", C.c_double)]
+    _fields_ = [(n, C.c_uint64) for n in _CNT] + [(n, C.c_double) for n in _TERMS] + [("absorbed_target", C.c_double), ("bias_gained", C.c_double),
+                                                                                   ("bias_lost", C.c_double)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -102,6 +103,11 @@ def oracle() -> C.CDLL:
         lib.oracle_detector_id.argtypes = [P(S.InputInfo), S.double3, S.double3, P(C.c_bool)]
         lib.oracle_kat_nearest_batch.restype = C.c_int
         lib.oracle_kat_nearest_batch.argtypes = [P(S.InputInfo), C.c_int, pd, D, C.c_int, pd, P(C.c_int), pd]
+        lib.oracle_weight_integral.restype = D
+        lib.oracle_weight_integral.argtypes = [D, D, D, C.c_uint]
+        lib.oracle_weight_tables.restype = C.c_int
+        lib.oracle_weight_tables.argtypes = [P(S.InputInfo)]
+        lib.oracle_free_weight_tables.argtypes = [P(S.InputInfo)]
         lib.oracle_kat_nearest.restype = C.c_int
         lib.oracle_kat_nearest.argtypes = [P(S.InputInfo), pd, pd, D, C.c_int, pd, P(C.c_int), pd]
         _oracle = lib
@@ -186,7 +192,11 @@ def ref_load_model(xml: str, surface: str, fast: bool = False) -> S.InputInfo:
         raise RuntimeError("reference ParseInputFile failed")
     if not lib.ref_parse_surface(surface.encode(), C.byref(info)):
         raise RuntimeError("reference ParseSurfaceFile failed")
-    lib.ref_dummy_weight_table(C.byref(info))
+    if info.useBiasing:  # the reference's own weight tables (weight_integral.cpp:34-65), as its launcher makes them
+        lib.ref_weight_tables.argtypes = [C.POINTER(S.InputInfo), C.c_int]
+        lib.ref_weight_tables(C.byref(info), os.cpu_count() or 1)
+    else:
+        lib.ref_dummy_weight_table(C.byref(info))
     return info
 
 

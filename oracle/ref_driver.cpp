@@ -23,8 +23,24 @@
 #include "launcher_omp.h"
 #include "parser.h"
 #include "writer.h"
+#include "weight_integral.h"
+
+// weight_integral.cpp:34-65 (external linkage, not declared in its header)
+void ComputeWeightIntegral(InputInfo* input, CmdArguments* args);
 
 extern "C" {
+
+/* mcml_integration.cpp:7-83: one weight-integral value */
+double ref_weight_integral(double dot, double g, double eps, unsigned n) { return ComputeWeightIntegral(dot, g, eps, n); }
+
+/* weight_integral.cpp:34-65: the weight tables of every distinct layer anisotropy, as the
+ * reference's launcher computes them before LaunchOMP when <Biasing> is on (no file written) */
+void ref_weight_tables(InputInfo* in, int nthreads) {
+    CmdArguments args;
+    memset(&args, 0, sizeof(args));
+    args.numberOfThreads = nthreads > 0 ? nthreads : 1;
+    ComputeWeightIntegral(in, &args);
+}
 
 int ref_parse_input(const char* xml, InputInfo* in) {
     memset(in, 0, sizeof(*in));

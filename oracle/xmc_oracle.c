@@ -67,6 +67,7 @@ typedef struct oracle_ledger {
     double specular, absorbed, absorbed_outside, escaped_top, escaped_bottom, lost_area, lost_cut,
         lost_glass, lost_budget, lost_invalid, roulette_killed, roulette_gained;
     double absorbed_target; /* weight dropped in layers flagged in targetRangeLayers (inside or outside Area) */
+    double bias_gained, bias_lost; /* weight added / removed by the biasing weight factor */
 } oracle_ledger;
 
 /* ------------------------------------------------------------------------ RNG: MCG59 */
@@ -702,6 +703,157 @@ static void o_absorb_outside(o_out* po, o_photon* ph, const InputInfo* in) {
     if (in->targetRangeLayers[ph->layer]) po->led.absorbed_target += dw;
 }
 
+/* ------------------------------------------------------------------------ biasing */
+
+/* mcml_kernel.cpp:325-364: the local attractive direction at the photon, the normalised
+ * difference of the fields of two point sources placed on the vertical through the target point:
+ * one l_tr above it, one l_tr + 2 delta below it (l_tr = 3D, D = 1 / (3 ((1 - g) mus + mua)),
+ * delta = 0.74 l_tr), positions relative to the start position. */
+static double3 o_attractive(const InputInfo* in, const o_photon* ph) {
+    const LayerInfo* L = &in->layerInfo[ph->layer];
+    double g = L->anisotropy, mus = L->scatteringCoefficient, mua = L->absorptionCoefficient;
+    double3 r = o_sub(ph->pos, in->startPosition);
+    double3 rd = o_sub(in->targetPoint, in->startPosition);
+    double diff = 1 / (3 * ((1 - g) * mus + mua));
+    double ltr = 3 * diff;
+    double delta = 0.74 * ltr;
+    double3 above = rd, below = rd;
+    above.z += ltr;
+    below.z -= ltr + 2 * delta;
+    double3 fa = o_sub(r, above);
+    double la = o_len(fa);
+    fa = o_div(fa, la * la * la);
+    double3 fb = o_sub(r, below);
+    double lb = o_len(fb);
+    fb = o_div(fb, lb * lb * lb);
+    return o_norm(o_sub(fb, fa));
+}
+
+/* mcml_kernel.cpp:430-440: the table of the layer's anisotropy (the last exact match) */
+static int o_weight_table(const InputInfo* in, double g) {
+    int found = -1;
+    for (int i = 0; i < in->numberOfWeightTables; ++i)
+        if (in->weightTable[i].anisotropy == g) found = i;
+    return found;
+}
+
+#define O_BIAS_MAX_TRIALS 65536u
+
+/* mcml_kernel.cpp:398-428: direction by rejection from HG with acceptance
+ * p = (0.1 + 0.9 (1 + d.v) / 2)^attractiveFactor, then weight *= W(d_old.v) / p with W from the
+ * weight-integral table (nearest node). MCG59: the draws are HG cos, azimuth, acceptance per trial,
+ * in that order. Philox: trial k uses the block of counter (id, iteration, 2 + k), slots 0, 1, 2;
+ * after O_BIAS_MAX_TRIALS trials the last candidate is taken (never reached for moderate factors). */
+static void o_biased_spin(const o_ctx* C, o_out* po, o_photon* ph, o_rng* rng) {
+    const InputInfo* in = C->in;
+    double g = in->layerInfo[ph->layer].anisotropy;
+    double3 v = o_attractive(in, ph);
+    double3 nd;
+    double p = 1.0;
+    for (uint32_t k = 0;; ++k) {
+        double u1, u2, u3;
+        if (rng->kind == ORACLE_RNG_PHILOX) {
+            uint32_t ctr[4] = {(uint32_t)rng->pid, (uint32_t)(rng->pid >> 32), rng->iter - 1u, 2u + k};
+            uint32_t out[4];
+            oracle_philox4x32_10(ctr, rng->key, out);
+            u1 = o_u24(out[0]); u2 = o_u24(out[1]); u3 = o_u24(out[2]);
+        } else {
+            u1 = oracle_mcg59_next(rng->mcg);
+            u2 = oracle_mcg59_next(rng->mcg);
+            u3 = oracle_mcg59_next(rng->mcg);
+        }
+        nd = oracle_spin(ph->dir, oracle_hg_cos(g, u1), u2);
+        p = 0.1 + 0.9 * ((1 + o_dot(nd, v)) / 2);
+        p = pow(p, in->attractiveFactor);
+        if (p > u3) break;
+        if (rng->kind == ORACLE_RNG_PHILOX && k + 1 >= O_BIAS_MAX_TRIALS) break;
+    }
+    int ti = o_weight_table(in, g);
+    if (ti >= 0) {
+        const WeightIntegralTable* T = &in->weightTable[ti];
+        double a = -1.0, b = 1.0;
+        int n = T->numberOfElements - 1;
+        double step = (b - a) / n;
+        double dot = o_dot(ph->dir, v);
+        int e = (int)floor((dot - a) / step + 0.5);
+        double nw = ph->weight * T->elements[e] / p;
+        if (nw > ph->weight) po->led.bias_gained += nw - ph->weight;
+        else po->led.bias_lost += ph->weight - nw;
+        ph->weight = nw;
+    }
+    ph->dir = nd;
+}
+
+/* mcml_integration.cpp:7-83: W(dot) = (1 / 2 pi) * integral over the sphere of the HG phase
+ * function about a direction at cosine `dot` to the attractive direction, times the acceptance
+ * (0.1 + 0.45 (1 + cos))^eps, by the product two-point Gauss-Legendre rule on n x n cells of
+ * (theta, phi) in [0, pi] x [0, 2 pi]. */
+double oracle_weight_integral(double dot, double g, double eps, unsigned n) {
+    const double coeff = 2.0 * sqrt(3.0);  /* Gauss nodes at the midpoint +- h / (2 sqrt 3) */
+    const double hx = O_PI / n, hy = 2 * O_PI / n;
+    const double g2 = g * g;
+    const double s = sqrt(1 - dot * dot);
+    double total = 0.0;
+    for (unsigned i = 0; i < n; ++i) {
+        double x0 = hx * i, x1 = x0 + hx;
+        double xs[2] = {0.5 * (x0 + x1) + (x1 - x0) / coeff, 0.5 * (x0 + x1) - (x1 - x0) / coeff};
+        for (unsigned j = 0; j < n; ++j) {
+            double y0 = hy * j, y1 = y0 + hy;
+            double ys[2] = {0.5 * (y0 + y1) + (y1 - y0) / coeff, 0.5 * (y0 + y1) - (y1 - y0) / coeff};
+            double cell = 0.0;
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) {
+                    double st = sin(xs[a]);
+                    double along = st * cos(ys[b]);                     /* cosine to the attractive direction */
+                    double c = dot * along + s * st * sin(ys[b]);       /* cosine to the photon direction */
+                    double q = 1 + g2 - 2 * g * c;
+                    double f = (1 - g2) / (2 * q * sqrt(q));
+                    cell += f * pow(0.1 + 0.9 * 0.5 * (1 + along), eps) * st;
+                }
+            total += 0.25 * (x1 - x0) * (y1 - y0) * cell;
+        }
+    }
+    return total / (2.0 * O_PI);
+}
+
+/* weight_integral.cpp:67-104 and :34-65: one table per distinct anisotropy of layers 1..L-1,
+ * weightTablePrecision + 1 nodes over dot in [-1, 1], integral precision scaled up for strongly
+ * forward-peaked layers. Tables are malloc'ed; free with oracle_free_weight_tables. */
+int oracle_weight_tables(InputInfo* in) {
+    double gs[MAX_LAYERS];
+    int ng = 0;
+    for (int l = 1; l < in->numberOfLayers; ++l) {
+        double g = in->layerInfo[l].anisotropy;
+        int seen = 0;
+        for (int k = 0; k < ng; ++k) if (gs[k] == g) seen = 1;
+        if (!seen) gs[ng++] = g;
+    }
+    in->numberOfWeightTables = ng;
+    in->weightTable = (WeightIntegralTable*)calloc((size_t)(ng > 0 ? ng : 1), sizeof(WeightIntegralTable));
+    for (int k = 0; k < ng; ++k) {
+        unsigned prec = in->weightIntegralPrecision;
+        if (gs[k] > 0.98) prec *= 16;
+        else if (gs[k] > 0.97) prec *= 8;
+        else if (gs[k] > 0.95) prec *= 4;
+        else if (gs[k] > 0.90) prec *= 2;
+        WeightIntegralTable* T = &in->weightTable[k];
+        T->anisotropy = gs[k];
+        T->numberOfElements = (int)in->weightTablePrecision + 1;
+        T->elements = (double*)malloc(sizeof(double) * (size_t)T->numberOfElements);
+        double step = 2.0 / in->weightTablePrecision;
+        for (int j = 0; j < T->numberOfElements; ++j)
+            T->elements[j] = oracle_weight_integral(-1.0 + j * step, gs[k], in->attractiveFactor, prec);
+    }
+    return ng;
+}
+
+void oracle_free_weight_tables(InputInfo* in) {
+    for (int k = 0; k < in->numberOfWeightTables; ++k) free(in->weightTable[k].elements);
+    free(in->weightTable);
+    in->weightTable = NULL;
+    in->numberOfWeightTables = 0;
+}
+
 /* mcml_kernel.cpp:39-126: one photon, start to death */
 static void o_photon_walk(const o_ctx* C, o_out* po, o_rng* rng, o_traj* tr) {
     const InputInfo* in = C->in;
@@ -760,8 +912,12 @@ static void o_photon_walk(const o_ctx* C, o_out* po, o_rng* rng, o_traj* tr) {
                     } else {
                         o_absorb_outside(po, &ph, in);
                     }
-                    double cost = oracle_hg_cos(L->anisotropy, o_draw(rng, 1));
-                    ph.dir = oracle_spin(ph.dir, cost, o_draw(rng, 2));
+                    if (in->useBiasing) {  /* mcml_kernel.cpp:108-109 */
+                        o_biased_spin(C, po, &ph, rng);
+                    } else {
+                        double cost = oracle_hg_cos(L->anisotropy, o_draw(rng, 1));
+                        ph.dir = oracle_spin(ph.dir, cost, o_draw(rng, 2));
+                    }
                 } else {
                     ph.dead = 1; po->led.n_area++; po->led.lost_area += ph.weight;
                 }
@@ -810,6 +966,7 @@ static void o_led_add(oracle_ledger* a, const oracle_ledger* b) {
     a->lost_budget += b->lost_budget; a->lost_invalid += b->lost_invalid;
     a->roulette_killed += b->roulette_killed; a->roulette_gained += b->roulette_gained;
     a->absorbed_target += b->absorbed_target;
+    a->bias_gained += b->bias_gained; a->bias_lost += b->bias_lost;
 }
 
 void oracle_default_opts(oracle_opts* o) {

@@ -42,7 +42,8 @@ def ledger_identity_fx(led: dict) -> int:
     for k in S.LEDGER_TERMS:
         v = led[k + "_fx"]
         tot += -v if k == "roulette_gained" else v
-    return tot
+    # biasing: weight created (gained) and removed (lost) by the weight-table factor
+    return tot - led.get("bias_gained_fx", 0) + led.get("bias_lost_fx", 0)
 
 
 def zscores(g, o, var_g, var_o):

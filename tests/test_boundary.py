@@ -244,7 +244,17 @@ def test_create_rejects_invalid_input_before_touching_the_device(tmp_path):
     xml, surf = sc.write(str(tmp_path), "bias")
     m = api.Model(xml, surf)
     m.info.useBiasing = 1
-    assert lib.xmc_create(C.byref(m.info), None, C.byref(ctx)) == S.XMC_ERR_UNSUPPORTED
+    m.info.attractiveFactor = -1.0
+    assert lib.xmc_create(C.byref(m.info), None, C.byref(ctx)) == S.XMC_ERR_INVALID_INPUT
+    m.info.attractiveFactor = 1.0
+    # caller tables without the anisotropy of a tissue layer (GetWeightTableIndex would find none)
+    tab = (S.WeightIntegralTable * 1)()
+    elems = (C.c_double * 3)(1.0, 1.0, 1.0)
+    tab[0].anisotropy, tab[0].numberOfElements, tab[0].elements = 0.123, 3, elems
+    m.info.weightTable, m.info.numberOfWeightTables = C.cast(tab, C.POINTER(S.WeightIntegralTable)), 1
+    assert lib.xmc_create(C.byref(m.info), None, C.byref(ctx)) == S.XMC_ERR_INVALID_INPUT
+    assert "weight table" in _lib.last_error()
+    m.info.weightTable, m.info.numberOfWeightTables = None, 0
     m.info.useBiasing = 0
     m.info.numberOfLayers = 9
     assert lib.xmc_create(C.byref(m.info), None, C.byref(ctx)) == S.XMC_ERR_RANGE

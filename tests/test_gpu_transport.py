@@ -354,3 +354,64 @@ def test_checkpoint_resume_bit_identical(tmp_path):
     for k in ("photons_launched", "steps", "absorbed_fx", "escaped_top_fx", "roulette_killed_fx", "roulette_gained_fx"):
         assert st.ledger[k] == whole_led[k], k
     t.close()
+
+
+def _biased_scene(n, factor=1.0, target=(1, 0, 2)):
+    sc = scenes.planar(photons=n, name="bias")
+    sc.time_start, sc.time_finish, sc.time_bins = 0.0, 30.0, 10
+    sc.bias_target, sc.bias_factor = target, factor
+    sc.bias_integral_precision, sc.bias_table_precision = 12, 512
+    return sc
+
+
+def test_weight_integral_tables_on_gpu(tmp_path):
+    """xmc_weight_integral_table (FP64 on the GPU) against the oracle's restatement of the reference's
+    quadrature (itself pinned bit for bit), including a layer with g > 0.95 (4x integral precision)."""
+    sc = _biased_scene(10, factor=1.7)
+    sc.layers[2].g = 0.96
+    xml, surf = sc.write(str(tmp_path), "wt")
+    m = api.Model(xml, surf)
+    _lib.check(_lib.load().xmc_weight_integral_table(C.byref(m.info), 0))
+    o = S.InputInfo.from_buffer_copy(m.info)
+    o.weightTable, o.numberOfWeightTables = None, 0
+    B.oracle().oracle_weight_tables(C.byref(o))
+    assert m.info.numberOfWeightTables == o.numberOfWeightTables == 3
+    worst = 0.0
+    for k in range(3):
+        a, b = m.info.weightTable[k], o.weightTable[k]
+        assert a.anisotropy == b.anisotropy and a.numberOfElements == b.numberOfElements == 513
+        ga = np.ctypeslib.as_array(a.elements, shape=(513,))
+        ob = np.ctypeslib.as_array(b.elements, shape=(513,))
+        worst = max(worst, float(np.max(np.abs(ga - ob) / np.abs(ob))))
+    print("weight tables max rel diff", worst)
+    assert worst < 1e-11
+    B.oracle().oracle_free_weight_tables(C.byref(o))
+
+
+@pytest.mark.parametrize("factor", [1.0, 3.0])
+def test_biasing_matches_oracle(tmp_path, factor):
+    """<Biasing> on (attractive point, weight tables computed on the GPU): rings and time bins within
+    3 sigma of the oracle, the fixed-point ledger (with the weight created and removed by the
+    biasing factor) closes exactly, and weights above 1 (factor 3) do not overflow."""
+    n = 60_000
+    sc = _biased_scene(n, factor=factor)
+    xml, surf = sc.write(str(tmp_path), f"b{int(factor)}")
+    m = api.Model(xml, surf)
+    _lib.check(_lib.load().xmc_weight_integral_table(C.byref(m.info), 0))
+    t = api.Transport(m, roulette=True)
+    led = t.run(n, seed=5)
+    tal = t.tallies()
+    out = api.Output(m)
+    oled, dw2, tw2 = B.oracle_run(m.info, out.info, oracle_opts_for(True, True, 0.0), seed=5, n=n)
+    t.close()
+    _check_exact(led, n)
+    assert led["bias_gained_fx"] > 0 and led["bias_lost_fx"] > 0
+    print(f"bias x{factor}: gained {led['bias_gained']:.4f} / {oled['bias_gained'] / n:.4f}, "
+          f"lost {led['bias_lost']:.4f} / {oled['bias_lost'] / n:.4f}")
+    z = _check_rings(tal, out, dw2, n, f"bias{factor}")
+    g = tal["time_weight"].astype(float) / WEIGHT_SCALE
+    zt = zscores(g, out.time_weights(), sum_var(g, tal["time_weight2"].astype(float) / WEIGHT_SCALE, n),
+                 sum_var(out.time_weights(), tw2, n))
+    assert np.all(np.abs(zt) < 3.0)
+    for k in ("bias_gained", "bias_lost"):
+        assert led[k] == pytest.approx(oled[k] / n, rel=0.05)

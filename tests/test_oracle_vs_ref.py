@@ -74,3 +74,38 @@ def test_pin_leapfrog_threads_reproduce_serial_sum(tmp_path):
     r = B.output_arrays(rout)
     assert r["specular"] == pytest.approx(((1 - 1.4) / (1 + 1.4)) ** 2)
     assert r["det_count"].sum() <= 3000
+
+
+def test_pin_weight_integral_and_tables(tmp_path):
+    """mcml_integration.cpp:7-83 and weight_integral.cpp:34-104, restated in the oracle: bit for bit."""
+    o, r = B.oracle(), B.ref()
+    r.ref_weight_integral.restype = C.c_double
+    r.ref_weight_integral.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint]
+    for dot in (-1.0, -0.71, 0.0, 0.33, 1.0):
+        for g, eps, n in ((0.0, 1.0, 8), (0.8, 1.0, 16), (0.93, 2.5, 12)):
+            assert o.oracle_weight_integral(dot, g, eps, n) == r.ref_weight_integral(dot, g, eps, n)
+    sc = scenes.planar(photons=10, name="wt")
+    sc.layers[2].g = 0.96  # two distinct anisotropies, one of them > 0.95 (4x integral precision)
+    sc.bias_target, sc.bias_integral_precision, sc.bias_table_precision, sc.bias_factor = (0, 0, 2), 8, 64, 1.5
+    xml, surf = sc.write(str(tmp_path))
+    rinfo = B.ref_load_model(xml, surf)
+    oinfo = B.ref_load_model(xml, surf)  # a second copy: the oracle recomputes its tables
+    oinfo.weightTable, oinfo.numberOfWeightTables = None, 0
+    assert o.oracle_weight_tables(C.byref(oinfo)) == rinfo.numberOfWeightTables == 3
+    for k in range(3):
+        a, b = rinfo.weightTable[k], oinfo.weightTable[k]
+        assert a.anisotropy == b.anisotropy and a.numberOfElements == b.numberOfElements == 65
+        assert all(a.elements[j] == b.elements[j] for j in range(65))
+    o.oracle_free_weight_tables(C.byref(oinfo))
+
+
+def test_pin_biasing(tmp_path):
+    """<Biasing> on: rejection-sampled directions towards the attractive point and the weight-table
+    correction (mcml_kernel.cpp:325-440), reproduced bit for bit."""
+    sc = scenes.planar(photons=1200, name="pin_bias")
+    sc.time_start, sc.time_finish, sc.time_bins = 0.0, 20.0, 8
+    sc.bias_target, sc.bias_integral_precision, sc.bias_table_precision, sc.bias_factor = (1, 0, 2), 8, 256, 1.0
+    xml, surf = sc.write(str(tmp_path))
+    ref, led = _pin(xml, surf, 1200)
+    assert led["bias_gained"] > 0 and led["bias_lost"] > 0
+    assert ref["det_weight"].sum() > 0

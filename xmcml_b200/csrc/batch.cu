@@ -100,7 +100,7 @@ __device__ __forceinline__ void lat(unsigned long long* p, unsigned long long v)
 }
 
 template <int kScheme>
-__global__ void __launch_bounds__(512, 1) batch_kernel(const BatchParams P) {
+__global__ void __launch_bounds__(256, 3) batch_kernel(const BatchParams P) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int n_inst = (int)P.hdr[0];
@@ -517,8 +517,8 @@ int occupancy(int scheme, int block, int* occ) {
 }
 
 int apply_tuning(xmc_batch* b, const xmc_batch_tuning& t) {
-    if (t.block_size < 32 || t.block_size > 512 || t.block_size % 32)
-        return bfail(XMC_ERR_INVALID_INPUT, "block_size must be a multiple of 32 in [32, 512]");
+    if (t.block_size < 32 || t.block_size > 256 || t.block_size % 32)
+        return bfail(XMC_ERR_INVALID_INPUT, "block_size must be a multiple of 32 in [32, 256]");
     if (t.photons_per_chunk < 1 || t.photons_per_chunk > (1 << 20))
         return bfail(XMC_ERR_INVALID_INPUT, "photons_per_chunk must be in [1, 2^20]");
     if (t.tally_scheme != 0 && t.tally_scheme != 1) return bfail(XMC_ERR_INVALID_INPUT, "tally_scheme must be 0 or 1");
@@ -763,7 +763,7 @@ extern "C" int xmc_batch_autotune(xmc_batch* b, const xmc_batch_instance* sample
     const xmc_batch_tuning keep = b->tuning;
     xmc_batch_tuning win{};
     win.ms = INFINITY;
-    const int blocks[] = {128, 256, 512};
+    const int blocks[] = {64, 128, 256};
     const int chunks[] = {32, 64, 128, 256};
     for (int scheme = 0; scheme < 2; ++scheme)
         for (int bs : blocks)

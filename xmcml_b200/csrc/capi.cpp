@@ -36,7 +36,7 @@ static void free_context(Context* c) {
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
                      c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
                      c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_z, c->d_cell_entries,
-                     c->d_big, c->d_cancel};
+                     c->d_big, c->d_cancel, c->d_wtab};
     for (void* p : dbufs)
         if (p) cudaFree(p);
     void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status};
@@ -99,7 +99,8 @@ static int validate(const InputInfo* in, const xmc_options& opt) {
     if (in->timeScaleSize < 1) return fail(XMC_ERR_INVALID_INPUT, "timeScaleSize must be >= 1");
     if ((long long)in->timeScaleSize * (in->numberOfCubeDetectors + in->numberOfRingDetectors) > (1ll << 26))
         return fail(XMC_ERR_RANGE, "time-bin tally too large");
-    if (in->useBiasing) return fail(XMC_ERR_UNSUPPORTED, "biasing (attractive point) is not provided by the GPU path");
+    if (in->useBiasing && !(std::isfinite(in->attractiveFactor) && in->attractiveFactor >= 0))
+        return fail(XMC_ERR_INVALID_INPUT, "attractiveFactor must be finite and >= 0");
     for (int l = 0; l < in->numberOfLayers; ++l) {
         const LayerInfo& L = in->layerInfo[l];
         if (L.numberOfSurfaces < 0 || (L.numberOfSurfaces > 0 && !L.surfaceId))
@@ -277,6 +278,58 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.grid_ny = img->grid.ny;
     kp.n_big = (int)(img->grid.big.size() / 4);
     img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next);
+    // ---- biasing (mcml_kernel.cpp:325-440) ----
+    kp.use_bias = in->useBiasing ? 1 : 0;
+    for (int l = 0; l < MAX_LAYERS; ++l) kp.layer_wtab[l] = -1;
+    if (kp.use_bias) {
+        kp.bias_eps = (float)in->attractiveFactor;
+        kp.bias_ox = (float)in->startPosition.x;
+        kp.bias_oy = (float)in->startPosition.y;
+        kp.bias_oz = (float)in->startPosition.z;
+        kp.bias_rx = (float)(in->targetPoint.x - in->startPosition.x);
+        kp.bias_ry = (float)(in->targetPoint.y - in->startPosition.y);
+        kp.bias_rz = (float)(in->targetPoint.z - in->startPosition.z);
+        if (in->weightTable && in->numberOfWeightTables > 0) {
+            // the caller's tables (the reference's launcher computes them before LaunchOMP)
+            const int ne = in->weightTable[0].numberOfElements;
+            std::vector<double> gs, tab;
+            for (int k = 0; k < in->numberOfWeightTables; ++k) {
+                const WeightIntegralTable& T = in->weightTable[k];
+                if (T.numberOfElements != ne || ne < 2 || !T.elements)
+                    return fail(XMC_ERR_INVALID_INPUT, "weight tables must share one element count >= 2");
+                gs.push_back(T.anisotropy);
+                tab.insert(tab.end(), T.elements, T.elements + ne);
+            }
+            st = set_weight_tables(in, gs, tab, ne, img);
+            if (st) return st;
+        } else {
+            img->need_wtab = true;
+        }
+    }
+    return XMC_OK;
+}
+
+// Layer -> table (GetWeightTableIndex, mcml_kernel.cpp:430-440: the last table whose anisotropy
+// equals the layer's) and the FP32 copy the kernel reads.
+int set_weight_tables(const InputInfo* in, const std::vector<double>& gs, const std::vector<double>& tables, int n_elem,
+                      HostImage* img) {
+    KParams& kp = img->kp;
+    for (int l = 0; l < MAX_LAYERS; ++l) kp.layer_wtab[l] = -1;
+    for (int l = 0; l < in->numberOfLayers; ++l) {
+        const LayerInfo& L = in->layerInfo[l];
+        int found = -1;
+        for (size_t k = 0; k < gs.size(); ++k)
+            if (gs[k] == L.anisotropy) found = (int)k;
+        const bool tissue = !(L.absorptionCoefficient == 0.0 && L.scatteringCoefficient == 0.0);
+        if (found < 0 && tissue && l > 0)
+            return fail(XMC_ERR_INVALID_INPUT, "no weight table for the anisotropy of layer " + std::to_string(l));
+        if (found > 127) return fail(XMC_ERR_RANGE, "too many weight tables");
+        kp.layer_wtab[l] = (int8_t)found;
+    }
+    img->wtab.resize(tables.size());
+    for (size_t i = 0; i < tables.size(); ++i) img->wtab[i] = (float)tables[i];
+    kp.wtab_n = n_elem;
+    img->need_wtab = false;
     return XMC_OK;
 }
 
@@ -325,6 +378,10 @@ void fill_ledger(const unsigned long long* L, uint32_t w0_fx, uint64_t n, xmc_le
     led->roulette_gained = (double)led->roulette_gained_fx * s;
     led->absorbed_target_fx = L[L_ABSORBED_TGT];
     led->absorbed_target = (double)led->absorbed_target_fx * s;
+    led->bias_gained_fx = L[L_BIAS_GAINED];
+    led->bias_lost_fx = L[L_BIAS_LOST];
+    led->bias_gained = (double)led->bias_gained_fx * s;
+    led->bias_lost = (double)led->bias_lost_fx * s;
 }
 
 static int create(const InputInfo* in, const xmc_options* opt_in, Context** out) {
@@ -332,6 +389,14 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     HostImage img;
     int st = prepare_image(in, opt_in, &img);
     if (st) return st;
+    if (img.need_wtab) {  // biasing without the caller's tables: compute them (weight_integral.cpp:34-65) on the GPU
+        std::vector<double> gs, tables;
+        int ne = 0;
+        st = compute_weight_tables(in, img.opt.device, &gs, &tables, &ne);
+        if (st) return st;
+        st = set_weight_tables(in, gs, tables, ne, &img);
+        if (st) return st;
+    }
     const xmc_options& opt = img.opt;
     const GeomImage& geom = img.geom;
     const std::vector<int8_t>& next = img.next;
@@ -382,6 +447,10 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     CK(up(&c->d_cell_z, img.grid.cell_z.data(), sizeof(float4) * img.grid.cell_z.size()));
     CK(up(&c->d_cell_entries, img.grid.entries.data(), sizeof(float4) * img.grid.entries.size()));
     CK(up(&c->d_big, img.grid.big.data(), sizeof(float4) * img.grid.big.size()));
+    if (img.kp.use_bias) {
+        CK(up(&c->d_wtab, img.wtab.data(), sizeof(float) * img.wtab.size()));
+        c->h2d_bytes += sizeof(float) * img.wtab.size();
+    }
     c->h2d_bytes += sizeof(uint2) * img.grid.cells.size() +
                     sizeof(float4) * (img.grid.cell_z.size() + img.grid.entries.size() + img.grid.big.size());
     const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
@@ -417,6 +486,7 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     kp.cell_z = (const float4*)c->d_cell_z;
     kp.cell_entries = (const float4*)c->d_cell_entries;
     kp.big = (const float4*)c->d_big;
+    kp.wtab = (const float*)c->d_wtab;
     kp.absorb = (unsigned long long*)c->d_absorb;
     kp.det = (unsigned long long*)c->d_det;
     kp.tbin = (unsigned long long*)c->d_tbin;
@@ -432,7 +502,7 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     c->block = opt.block_size > 0 ? opt.block_size : 256;
     if (c->block % 32 != 0 || c->block > 1024) return bail(fail(XMC_ERR_INVALID_INPUT, "block_size must be a multiple of 32 <= 1024"));
     int occ = 0;
-    CK(transport_occupancy(c->block, c->smem_bytes, &occ));
+    CK(transport_occupancy(c->block, c->smem_bytes, &occ, c->kp.use_bias != 0));
     if (occ <= 0) return bail(fail(XMC_ERR_DEVICE, "transport kernel cannot be resident with this block size / shared memory"));
     c->blocks_per_sm = opt.blocks_per_sm > 0 ? std::min(opt.blocks_per_sm, occ) : occ;
     c->grid = c->num_sms * c->blocks_per_sm;

@@ -393,6 +393,10 @@ void xmc_free_input(InputInfo* in) {
     }
     delete[] in->cubeDetector;
     delete[] in->ringDetector;
+    if (in->weightTable) {
+        for (int k = 0; k < in->numberOfWeightTables; ++k) delete[] in->weightTable[k].elements;
+        delete[] in->weightTable;
+    }
     std::memset(in, 0, sizeof(*in));
 }
 

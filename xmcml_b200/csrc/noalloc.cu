@@ -66,6 +66,10 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     HostImage img;
     int st = prepare_image(input, opt, &img);
     if (st) return st;
+    if (img.kp.use_bias) {
+        set_error("xmc_run_noalloc: biasing needs weight tables this entry point does not stage");
+        return XMC_ERR_UNSUPPORTED;
+    }
     if (img.opt.flags & (XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ)) {
         set_error("xmc_run_noalloc: scattering and trajectory maps need buffers this entry point does not take");
         return XMC_ERR_UNSUPPORTED;

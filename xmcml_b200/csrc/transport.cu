@@ -16,6 +16,7 @@
 // (weight 1.0 == 2^31): every deposit is subtracted from the photon's integer weight, so the
 // ledger terms add up to launched weight exactly.
 #include <cstdint>
+#include <type_traits>
 
 #include "geom.cuh"
 #include "photon.cuh"
@@ -27,10 +28,13 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Photon weight in 2^31 fixed point: 32 bits (weight <= 1 always holds without biasing) or 64 bits
+// (the biasing factor W / p can raise a weight above 1).
+template <typename WT>
 struct Photon {
     float px, py, pz, dx, dy, dz;
     float time, trange, orange;
-    uint32_t w;
+    WT w;
     int layer;
     uint32_t visited;
     uint32_t iter;
@@ -40,6 +44,15 @@ struct Photon {
     int rdet;              // replay pass: the detector this photon reached in the run pass
     unsigned long long pid;
 };
+
+__device__ __forceinline__ float w2f(uint32_t w) { return __uint2float_rn(w); }
+__device__ __forceinline__ float w2f(unsigned long long w) { return __ull2float_rn(w); }
+template <typename WT> __device__ __forceinline__ WT f2w(float f);
+template <> __device__ __forceinline__ uint32_t f2w<uint32_t>(float f) { return __float2uint_rn(f); }
+template <> __device__ __forceinline__ unsigned long long f2w<unsigned long long>(float f) { return __float2ull_rn(f); }
+// w^2 in fixed point ((w w) >> 31), exact for weights below 2^32 in weight units
+__device__ __forceinline__ unsigned long long wsq(uint32_t w) { return ((unsigned long long)w * w) >> 31; }
+__device__ __forceinline__ unsigned long long wsq(unsigned long long w) { return (__umul64hi(w, w) << 33) | ((w * w) >> 31); }
 
 // The triangle-free z-gap around z: (highest occupied top below z, lowest occupied bottom above
 // z), or an empty interval when z lies inside an occupied slab.
@@ -83,7 +96,8 @@ __device__ __forceinline__ void lat(unsigned long long* p, unsigned long long v)
 
 // mcml_kernel.cpp:663-742 (first matching cube, then ring; layer filter; angle test) and the
 // detector tallies of :744-858. Weight arithmetic in fixed point.
-__device__ int find_detector(const KParams& P, const DevDetector* __restrict__ s_det, const Photon& ph) {
+template <class Ph>
+__device__ int find_detector(const KParams& P, const DevDetector* __restrict__ s_det, const Ph& ph) {
     int det = -1;
     const float l2 = ph.dx * ph.dx + ph.dy * ph.dy + ph.dz * ph.dz;
     const float ac = -ph.dz / l2;
@@ -122,11 +136,13 @@ __device__ int find_detector(const KParams& P, const DevDetector* __restrict__ s
     return det;
 }
 
-__device__ void tally_detection(const KParams& P, const SmemTally& S, const Photon& ph, int det) {
-    const uint32_t w = ph.w;
+template <class Ph>
+__device__ void tally_detection(const KParams& P, const SmemTally& S, const Ph& ph, int det) {
+    using WT = decltype(ph.w);
+    const WT w = ph.w;
     const float total = ph.trange + ph.orange;
-    const uint32_t tw = total > 0.0f ? __float2uint_rn(__uint2float_rn(w) * (ph.trange / total)) : 0u;
-    const unsigned long long w2 = ((unsigned long long)w * w) >> 31;
+    const WT tw = total > 0.0f ? f2w<WT>(w2f(w) * (ph.trange / total)) : (WT)0;
+    const unsigned long long w2 = wsq(w);
     atomicAdd(&S.det[4 * det + 0], (unsigned long long)w);
     atomicAdd(&S.det[4 * det + 1], 1ull);
     lat(&S.det[4 * det + 2], tw);
@@ -152,8 +168,8 @@ __device__ void tally_detection(const KParams& P, const SmemTally& S, const Phot
 // weight to the scattering map there; the replay pass counts the crossing in the trajectory map of
 // the detector the photon reaches (UpdateDetectorTrajectory, :794-810), which the reference does by
 // replaying a per-photon crossing log at detection.
-__device__ void cross_planes(const KParams& P, float x0, float y0, float z0, float x1, float y1, float z1, uint32_t w,
-                             int rdet) {
+__device__ void cross_planes(const KParams& P, float x0, float y0, float z0, float x1, float y1, float z1,
+                             unsigned long long w, int rdet) {
     if (z1 == z0) return;
     float sx = x0, sy = y0, sz = z0, fz = z1, ex = x1 - x0, ey = y1 - y0, ez = z1 - z0;
     if (z1 < z0) {
@@ -177,14 +193,16 @@ __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, flo
     }
 }
 
-__device__ __forceinline__ void kill(const SmemTally& S, Photon& ph, bool& alive, int count_slot, int weight_slot) {
+template <class Ph>
+__device__ __forceinline__ void kill(const SmemTally& S, Ph& ph, bool& alive, int count_slot, int weight_slot) {
     atomicAdd(&S.ledger[count_slot], 1ull);
     lat(&S.ledger[weight_slot], ph.w);
     atomicAdd(&S.ledger[L_TERMINATED], 1ull);
     alive = false;
 }
 
-__device__ __forceinline__ void launch_photon(const KParams& P, Photon& ph, unsigned long long pid) {
+template <class Ph>
+__device__ __forceinline__ void launch_photon(const KParams& P, Ph& ph, unsigned long long pid) {
     ph.pid = pid;
     ph.px = P.sx;
     ph.py = P.sy;
@@ -213,9 +231,57 @@ __device__ __forceinline__ void launch_photon(const KParams& P, Photon& ph, unsi
     ph.tmin = kTminAfter;
 }
 
+constexpr uint32_t kBiasMaxTrials = 65536;
+
+// ComputePhotonDirectionWithBiasing (mcml_kernel.cpp:398-428): the local attractive direction v
+// (GetLocalAttractiveVector, :325-364: normalised difference of the fields of two point sources on
+// the vertical through the target point, l_tr above it and l_tr + 2 delta below it), a new direction
+// by rejection from HG with acceptance p = (0.1 + 0.45 (1 + d.v))^attractiveFactor (trial k draws the
+// Philox block (id, iteration, 2 + k): slot 0 cos theta, slot 1 azimuth, slot 2 acceptance), and
+// the weight factor W(d_old.v) / p from the layer's weight-integral table (nearest node).
+template <class Ph>
+__device__ __forceinline__ void biased_spin(const KParams& P, const DevLayer& L, int layer, Ph& ph,
+                                            unsigned long long& gained, unsigned long long& lost) {
+    using WT = decltype(ph.w);
+    const float ltr = 3.0f * (1.0f / (3.0f * ((1.0f - L.g) * L.mus + L.mua)));
+    const float delta = 0.74f * ltr;
+    const float rx = ph.px - P.bias_ox, ry = ph.py - P.bias_oy, rz = ph.pz - P.bias_oz;
+    const float ex = rx - P.bias_rx, ey = ry - P.bias_ry;
+    const float az = rz - (P.bias_rz + ltr), bz = rz - (P.bias_rz - ltr - 2.0f * delta);
+    const float ia = rsqrtf(ex * ex + ey * ey + az * az), ib = rsqrtf(ex * ex + ey * ey + bz * bz);
+    const float ca = ia * ia * ia, cb = ib * ib * ib;
+    float vx = ex * (cb - ca), vy = ey * (cb - ca), vz = bz * cb - az * ca;
+    const float vn = rsqrtf(vx * vx + vy * vy + vz * vz);
+    vx *= vn; vy *= vn; vz *= vn;
+    const float dot0 = ph.dx * vx + ph.dy * vy + ph.dz * vz;
+    float nx = ph.dx, ny = ph.dy, nz = ph.dz, p = 1.0f;
+    for (uint32_t k = 0; k < kBiasMaxTrials; ++k) {
+        const uint4 r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter - 1u, 2u + k),
+                                      P.key0, P.key1);
+        nx = ph.dx; ny = ph.dy; nz = ph.dz;
+        hg_spin(L.hg_a, L.hg_b, L.hg_c, L.hg_d, L.hg_e, u24(r.x), u24(r.y), nx, ny, nz);
+        p = powf(fmaf(0.45f, 1.0f + (nx * vx + ny * vy + nz * vz), 0.1f), P.bias_eps);
+        if (p > u24(r.z)) break;
+    }
+    const int t = P.layer_wtab[layer];
+    if (t >= 0) {
+        const float step = 2.0f / (float)(P.wtab_n - 1);
+        int e = (int)floorf((dot0 + 1.0f) / step + 0.5f);
+        e = min(max(e, 0), P.wtab_n - 1);
+        const float W = __ldg(&P.wtab[(size_t)t * P.wtab_n + e]);
+        const WT nw = f2w<WT>(w2f(ph.w) * (W / p));
+        if (nw > ph.w) gained += nw - ph.w;
+        else lost += ph.w - nw;
+        ph.w = nw;
+    }
+    ph.dx = nx; ph.dy = ny; ph.dz = nz;
+}
+
 }  // namespace
 
+template <bool kBias>
 __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
+    using WT = typename std::conditional<kBias, unsigned long long, uint32_t>::type;
     extern __shared__ __align__(16) unsigned char smem[];
     // --- shared memory carve-up (must match smem_layout on the host) ---
     unsigned long long* s_ledger = reinterpret_cast<unsigned long long*>(smem);
@@ -251,8 +317,9 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     unsigned long long cbeg = 0, cend = 0;  // warp-uniform chunk of photon indices
     bool exhausted = false;                 // warp-uniform
     bool alive = false;
-    Photon ph;
+    Photon<WT> ph;
     unsigned steps = 0, retests = 0, n_visit = 0, n_tri = 0;
+    unsigned long long bias_gained = 0, bias_lost = 0;
     unsigned long long absorbed = 0, absorbed_out = 0, absorbed_tgt = 0;  // per-thread sums, flushed at the end
     unsigned budget_hit = 0;
 
@@ -419,7 +486,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             ph.tmin = kTminAfter;
         } else {
             // ---- drop (mcml_kernel.cpp:633-642) ----
-            uint32_t dw = __float2uint_rn(__uint2float_rn(ph.w) * L.absorb);
+            WT dw = f2w<WT>(w2f(ph.w) * L.absorb);
             dw = min(dw, ph.w);
             ph.w -= dw;
             if (idx >= 0) {
@@ -430,7 +497,11 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             }
             if ((P.target_mask >> ph.layer) & 1u) absorbed_tgt += dw;
             // ---- spin (mcml_kernel.cpp:442-495) ----
-            hg_spin(L.hg_a, L.hg_b, L.hg_c, L.hg_d, L.hg_e, u24(r.y), u24(r.z), ph.dx, ph.dy, ph.dz);
+            if constexpr (kBias) {  // mcml_kernel.cpp:108-109
+                biased_spin(P, L, ph.layer, ph, bias_gained, bias_lost);
+            } else {
+                hg_spin(L.hg_a, L.hg_b, L.hg_c, L.hg_d, L.hg_e, u24(r.y), u24(r.z), ph.dx, ph.dy, ph.dz);
+            }
             ph.excl = -1;
             ph.tmin = 0.0f;
         }
@@ -440,7 +511,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                 if (ph.w == 0u) {
                     kill(S, ph, alive, L_N_ROULETTE, L_RKILLED);
                 } else if (u_roulette < P.chance) {
-                    const uint32_t nw = min(__float2uint_rn(__uint2float_rn(ph.w) * P.inv_chance), kWeightOne);
+                    const WT nw = min(f2w<WT>(w2f(ph.w) * P.inv_chance), (WT)kWeightOne);
                     lat(&S.ledger[L_RGAINED], nw - ph.w);
                     ph.w = nw;
                 } else {
@@ -457,6 +528,10 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     lat(&S.ledger[L_ABSORBED], absorbed);
     lat(&S.ledger[L_ABSORBED_OUT], absorbed_out);
     lat(&S.ledger[L_ABSORBED_TGT], absorbed_tgt);
+    if (kBias) {
+        lat(&S.ledger[L_BIAS_GAINED], bias_gained);
+        lat(&S.ledger[L_BIAS_LOST], bias_lost);
+    }
     if (retests) atomicAdd(&S.ledger[L_N_RETEST], (unsigned long long)retests);
     atomicAdd(&S.ledger[L_N_NODES], (unsigned long long)n_visit);
     atomicAdd(&S.ledger[L_N_TRIS], (unsigned long long)n_tri);
@@ -472,21 +547,29 @@ __global__ void philox_probe_kernel(uint32_t k0, uint32_t k1, unsigned long long
 }
 
 cudaError_t enqueue_transport(Context* ctx) {
-    transport_kernel<<<ctx->grid, ctx->block, ctx->smem_bytes, ctx->stream>>>(ctx->kp);
+    if (ctx->kp.use_bias)
+        transport_kernel<true><<<ctx->grid, ctx->block, ctx->smem_bytes, ctx->stream>>>(ctx->kp);
+    else
+        transport_kernel<false><<<ctx->grid, ctx->block, ctx->smem_bytes, ctx->stream>>>(ctx->kp);
     return cudaGetLastError();
 }
 
-cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm) {
+template <bool kBias>
+static cudaError_t occupancy_of(int block, size_t smem, int* blocks_per_sm) {
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, transport_kernel);
+    cudaError_t e = cudaFuncGetAttributes(&fa, transport_kernel<kBias>);
     if (e != cudaSuccess) return e;
     if (block > fa.maxThreadsPerBlock) {
         *blocks_per_sm = 0;
         return cudaSuccess;
     }
-    e = cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(transport_kernel<kBias>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel, block, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<kBias>, block, smem);
+}
+
+cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm, bool bias) {
+    return bias ? occupancy_of<true>(block, smem, blocks_per_sm) : occupancy_of<false>(block, smem, blocks_per_sm);
 }
 
 cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n, uint32_t* host_out) {

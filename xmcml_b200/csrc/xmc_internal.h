@@ -63,7 +63,7 @@ enum LedgerSlot {
     L_N_TOP, L_N_BOTTOM, L_N_AREA, L_N_CUT, L_N_ROULETTE, L_N_GLASS, L_N_BUDGET, L_N_INVALID,
     L_N_DETECTED, L_N_RETEST, L_N_NODES, L_N_TRIS,
     L_ABSORBED, L_ABSORBED_OUT, L_TOP, L_BOTTOM, L_AREA, L_CUT, L_GLASS, L_BUDGET, L_INVALID,
-    L_RKILLED, L_RGAINED, L_N_REPLAY_MISMATCH, L_ABSORBED_TGT,
+    L_RKILLED, L_RGAINED, L_N_REPLAY_MISMATCH, L_ABSORBED_TGT, L_BIAS_GAINED, L_BIAS_LOST,
     L_COUNT
 };
 constexpr int kLedgerSlots = 32;  // padded
@@ -143,6 +143,14 @@ struct KParams {
     unsigned long long* counter;  // photon id dispenser
     const volatile int* cancel;   // device cancel flag, written by xmc_cancel from another stream (may be null)
     int* status;                  // device status word: bit0 budget hit, bit1 cancelled
+    // biasing (InputInfo.useBiasing): attractive point and weight-integral tables
+    int use_bias;
+    float bias_eps;                       // attractiveFactor
+    float bias_ox, bias_oy, bias_oz;      // startPosition
+    float bias_rx, bias_ry, bias_rz;      // targetPoint - startPosition
+    const float* wtab;                    // [tables x wtab_n]
+    int wtab_n;                           // elements per table
+    int8_t layer_wtab[MAX_LAYERS];        // table of each layer's anisotropy, -1 if none
 };
 
 // Host-side device image and buffers of one context.
@@ -162,6 +170,7 @@ struct Context {
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
     void* d_counter = nullptr; void* d_status = nullptr;
     void* d_cells = nullptr; void* d_cell_z = nullptr; void* d_cell_entries = nullptr; void* d_big = nullptr; void* d_cancel = nullptr;
+    void* d_wtab = nullptr;
     cudaStream_t cancel_stream = nullptr;
     void* d_scatter = nullptr; void* d_traj = nullptr; void* d_replay = nullptr; void* d_replay_count = nullptr;
     void* d_replay_ledger = nullptr;
@@ -200,6 +209,8 @@ struct HostImage {
     KParams kp{};
     GeomImage geom;
     std::vector<int8_t> next;        // [n_surf * MAX_LAYERS]
+    std::vector<float> wtab;         // weight-integral tables (biasing)
+    bool need_wtab = false;          // biasing without caller tables: compute them on the GPU
     std::vector<DevDetector> dets;   // [max(1, n_dets)]
     GridImage grid;
     double rsp = 0.0;
@@ -207,6 +218,14 @@ struct HostImage {
     int grid_size = 0, n_dets = 0, n_time = 0;
     size_t smem_bytes = 0;
 };
+
+// weight_table.cu: weight-integral tables of the biased walk, computed on `device` in FP64
+int compute_weight_tables(const InputInfo* in, int device, std::vector<double>* gs, std::vector<double>* tables,
+                          int* n_elem);
+std::vector<double> distinct_anisotropies(const InputInfo* in);
+// capi.cpp: layer -> table mapping and float tables for the kernel from FP64 tables
+int set_weight_tables(const InputInfo* in, const std::vector<double>& gs, const std::vector<double>& tables, int n_elem,
+                      HostImage* img);
 
 // capi.cpp: validate `in` and build its host image (options normalised as xmc_create does).
 int prepare_image(const InputInfo* in, const xmc_options* opt, HostImage* img);
@@ -224,7 +243,7 @@ void build_xy_grid(const GeomImage& g, GridImage* out);
 // transport.cu: enqueue one transport kernel launch on ctx->stream (tallies must be zeroed).
 cudaError_t enqueue_transport(Context* ctx);
 // transport.cu: occupancy of the kernel for a block size and dynamic shared memory.
-cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm);
+cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm, bool bias = false);
 // transport.cu: Philox blocks computed on the device (self test).
 cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n, uint32_t* host_out);
 

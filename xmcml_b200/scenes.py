@@ -63,6 +63,11 @@ class Scene:
     start_position: Optional[Tuple[float, float, float]] = None
     start_direction: Optional[Tuple[float, float, float]] = None
     target_layers: Optional[List[int]] = None
+    # <Biasing>: attractive point (integers: the reference parses it with atoi) and weight integral
+    bias_target: Optional[Tuple[int, int, int]] = None
+    bias_factor: float = 1.0
+    bias_integral_precision: int = 128
+    bias_table_precision: int = 262144
     name: str = "scene"
 
     # ------------------------------------------------------------------ writers
@@ -84,6 +89,14 @@ class Scene:
             return [f"{ind}<{tag}>", f"{ind}    <X>{v[0]!r}</X>", f"{ind}    <Y>{v[1]!r}</Y>",
                     f"{ind}    <Z>{v[2]!r}</Z>", f"{ind}</{tag}>"]
 
+        if self.bias_target is not None:
+            out += ["    <Biasing>", "        <WeightIntegral>",
+                    f"            <IntegralPrecision>{int(self.bias_integral_precision)}</IntegralPrecision>",
+                    f"            <TablePrecision>{int(self.bias_table_precision)}</TablePrecision>",
+                    f"            <AttractiveFactor>{float(self.bias_factor)!r}</AttractiveFactor>",
+                    "        </WeightIntegral>", "        <TargetPoint>"]
+            out += [f"            <{a}>{int(v)}</{a}>" for a, v in zip("XYZ", self.bias_target)]
+            out += ["        </TargetPoint>", "    </Biasing>"]
         if self.start_position is not None:
             out += xyz("StartPosition", [float(x) for x in self.start_position])
         if self.start_direction is not None:

@@ -1,7 +1,7 @@
 """Train the surrogate on batched Monte Carlo tallies and judge it against high-photon Monte Carlo.
 
-    python -m xmcml_b200.surrogate_study --train 20000 --train-photons 200000 --test 200 \\
-        --test-photons 10000000 --out result.json
+    python -m xmcml_b200.surrogate_study --train 20000 --train-photons 1000000 --test 200 \\
+        --test-photons 10000000 --steps 30000 --out result.json
 
 1. Samples `train` + `test` instances of the layered sweep (per layer mua log-uniform [0.005, 1],
    mus [5, 40], g [0.7, 0.95], n [1.33, 1.45]; L1 / L2 thickness [0.05, 0.3] / [0.5, 2] mm; beam
@@ -40,18 +40,18 @@ def run_batched(b: XB.Batch, inst: XB.Instances, chunk: int):
 def main(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--train", type=int, default=20000)
-    p.add_argument("--train-photons", type=float, default=2e5)
+    p.add_argument("--train-photons", type=float, default=1e6)
     p.add_argument("--test", type=int, default=200)
     p.add_argument("--test-photons", type=float, default=1e7)
     p.add_argument("--members", type=int, default=4)
-    p.add_argument("--steps", type=int, default=6000)
+    p.add_argument("--steps", type=int, default=30000)
     p.add_argument("--batch", type=int, default=4096)
     p.add_argument("--lr", type=float, default=2e-3)
-    p.add_argument("--floor", type=float, default=1e-8)
+    p.add_argument("--floor", type=float, default=1e-7)
     p.add_argument("--gate", type=float, default=0.05)
     p.add_argument("--seed", type=int, default=2024)
     p.add_argument("--device", type=int, default=0)
-    p.add_argument("--weighted", action="store_true")
+    p.add_argument("--unweighted", action="store_true", help="plain (unweighted) mean squared error")
     p.add_argument("--out", default="")
     a = p.parse_args(argv)
 
@@ -71,7 +71,7 @@ def main(argv=None):
                        gate=a.gate)
     t0 = time.perf_counter()
     curves = sur.fit(train.features(), SG.reflectance_targets(rt_tr, a.floor), steps=a.steps, batch=a.batch, lr=a.lr,
-                     seed=a.seed, weighted=a.weighted)
+                     seed=a.seed, weighted=not a.unweighted)
     t_fit = time.perf_counter() - t0
     pred = sur.predict(test.features())
     err = SG.relative_error(pred["log10_r"], rt_te, w2_te, test.photons, floor=a.floor, max_ref_rse=0.01)
@@ -89,7 +89,7 @@ def main(argv=None):
     evals = 65536 / (ms_fwd / 1e3) / a.members
     mc_rate = float(test.photons.sum()) / (ms_te / 1e3)
     res = {
-        "weighted_loss": a.weighted, "floor": a.floor, "train_instances": a.train, "train_photons": a.train_photons, "test_instances": a.test,
+        "weighted_loss": not a.unweighted, "floor": a.floor, "train_instances": a.train, "train_photons": a.train_photons, "test_instances": a.test,
         "test_photons": a.test_photons, "members": a.members, "steps": a.steps, "batch": a.batch,
         "autotune": tune,
         "mc_train_photons_per_s": float(train.photons.sum()) / (ms_tr / 1e3), "mc_train_wall_s": t_gen,

@@ -80,3 +80,11 @@ def test_struct_sizes_match_the_header():
     assert C.sizeof(S.BatchInstance) == 280
     assert C.sizeof(S.BatchTuning) == 24
     assert C.sizeof(S.BatchResult) == 112
+
+
+def test_features_round_trip():
+    a = XB.sample_instances(8, 16, beam_radius=(0.0, 0.5))
+    b = XB.from_features(a.features(), photons=7, seed=100)
+    for k in ("mua", "mus", "g", "n", "thickness", "beam_radius"):
+        assert np.allclose(getattr(a, k), getattr(b, k), rtol=1e-12), k
+    assert np.all(b.photons == 7) and list(b.seed[:2]) == [100, 101]

@@ -174,3 +174,46 @@ def test_surrogate_beats_equal_cost_monte_carlo():
     assert np.all(np.isfinite(res["reflectance"]))
     sur.close()
     b.close()
+
+
+def test_inverse_fit_with_network_and_monte_carlo_check():
+    """The network stands in for the Monte Carlo inside an inverse fit: the absorption and scattering
+    coefficients of a held-out 3-layer instance are recovered from its Monte Carlo reflectance by a
+    search over network evaluations, and the Monte Carlo of the fitted properties reproduces the
+    target about as well as the Monte Carlo of the true ones. With a gate that rejects every query
+    the Monte Carlo ranks the search's best candidates instead (the fallback)."""
+    import time
+    from xmcml_b200 import batch as XB
+
+    rings, times = 10, 4
+    b = XB.Batch(n_rings=rings, n_time=times, ring_width=0.2, time_finish=1000 * 0.299792458, max_instances=4096)
+    train = XB.sample_instances(111, 3000, budget=(20000, 20000))
+    ytr = SG.reflectance_targets(b.run(train)["ring_time"], floor=1e-6)
+    sur = SG.Surrogate(n_in=15, n_out=rings * times, members=2, max_rows=8192, floor=1e-6, gate=1.0, gate_floor=1e-4)
+    sur.fit(train.features(), ytr, steps=1500, batch=1024, lr=2e-3, weighted=True)
+    truth = XB.sample_instances(313, 1, budget=(4_000_000, 4_000_000))
+    target = np.log10(b.run(truth)["ring_time"].reshape(-1) + 1e-6)
+    mask = target > np.log10(1e-4)
+    f_true = truth.features()[0]
+
+    def mc_loss(features, photons=200_000, seed=9):
+        r = b.run(XB.from_features(features[None, :], photons=photons, seed=seed))["ring_time"].reshape(-1)
+        return float(np.mean((np.log10(r[mask] + 1e-6) - target[mask]) ** 2))
+
+    free = list(range(6))  # log10 mua and mus of the three layers
+    t0 = time.perf_counter()
+    fit = sur.inverse_fit(target, f_true, free, pop=4096, iters=12, seed=3, batch=b, verify_photons=200_000)
+    t_fit = time.perf_counter() - t0
+    prior = f_true.copy()
+    prior[free] = sur.x_mean[free]
+    l_truth, l_prior = mc_loss(f_true), mc_loss(prior)
+    print(f"inverse fit: {fit['network_evals']} network evals in {t_fit:.2f} s; MC misfit fitted {fit['loss_mc']:.2e}, "
+          f"truth {l_truth:.2e}, prior {l_prior:.2e}; true mua {10 ** f_true[:3]}, fitted {10 ** fit['features'][:3]}")
+    assert fit["gated"] and fit["mc_evals"] == 1
+    assert fit["loss_mc"] < 3 * l_truth + 1e-3
+    assert fit["loss_mc"] < 0.3 * l_prior
+    sur.gate = 0.0  # every query fails the gate: the Monte Carlo picks among the search's best
+    fb = sur.inverse_fit(target, f_true, free, pop=2048, iters=6, seed=4, batch=b, verify_photons=100_000, refine=8)
+    assert not fb["gated"] and fb["mc_evals"] == 9 and np.isfinite(fb["loss_mc"])
+    sur.close()
+    b.close()

@@ -84,6 +84,17 @@ def make_instances(mua, mus, g, n, thickness, photons, seed, beam_radius=0.0, n_
                      v(beam_radius), v(n_above), v(n_below))
 
 
+def from_features(features: np.ndarray, photons: int, seed: int = 0, last_thickness: float = 50.0,
+                  n_ambient: float = 1.0) -> Instances:
+    """Inverse of Instances.features() for 3-layer instances: [log10 mua x3, mus x3, g x3, n x3,
+    L1 and L2 thickness, beam radius] -> instance table (L3 `last_thickness`)."""
+    f = np.atleast_2d(np.asarray(features, dtype=np.float64))
+    K = f.shape[0]
+    th = np.concatenate([f[:, 12:14], np.full((K, 1), last_thickness)], axis=1)
+    return make_instances(10 ** f[:, 0:3], f[:, 3:6], f[:, 6:9], f[:, 9:12], th, photons,
+                          np.uint64(seed) + np.arange(K, dtype=np.uint64), f[:, 14], n_ambient, n_ambient)
+
+
 def sample_instances(seed: int, count: int = 1024, budget=(1e5, 1e7), beam_radius=(0.0, 0.0),
                      last_thickness: float = 50.0) -> Instances:
     """`count` 3-layer instances drawn with numpy.random.default_rng(seed): per layer mua

@@ -282,6 +282,66 @@ class Surrogate:
                 b.close()
         return {"reflectance": r, "from_network": p["use_network"], "spread": p["spread"]}
 
+    # ---- inverse fitting ----
+    def mean_log10(self, features: np.ndarray) -> np.ndarray:
+        """Ensemble mean of log10 reflectance (no gate), for search loops."""
+        xs = ((np.asarray(features, dtype=np.float64) - self.x_mean) / self.x_std).astype(np.float32)
+        acc = None
+        for m in self.members:
+            y, _ = m.forward(xs)
+            y = y.astype(np.float64) * self.y_std + self.y_mean
+            acc = y if acc is None else acc + y
+        return acc / len(self.members)
+
+    def inverse_fit(self, target_log10: np.ndarray, start: np.ndarray, free: List[int], pop: int = 8192,
+                    iters: int = 15, elite: float = 0.02, seed: int = 0, batch=None, verify_photons: int = 0,
+                    refine: int = 16) -> Dict[str, object]:
+        """Fit the `free` input features to a measured log10 reflectance with the network standing in for
+        the Monte Carlo: a cross-entropy search (`pop` candidates per round, the best `elite` share
+        refits a Gaussian), candidates kept inside the training hull, misfit = mean squared log10
+        difference over the cells where the target is above gate_floor. With verify_photons > 0 the
+        batched Monte Carlo checks the winner; when the winner fails the gate (ensemble spread), the
+        Monte Carlo also ranks the `refine` best candidates of the last round and picks the best."""
+        rng = np.random.default_rng(seed)
+        t = np.asarray(target_log10, dtype=np.float64).ravel()
+        mask = t > np.log10(max(self.gate_floor, self.floor))
+        free = list(free)
+        base = np.asarray(start, dtype=np.float64).copy()
+        mu = self.x_mean[free].copy()
+        sd = self.x_std[free].copy()
+        lo, hi = self.lo[free], self.hi[free]
+        best, best_loss, hist, evals = base.copy(), np.inf, [], 0
+        cand = None
+        for it in range(iters):
+            cand = np.repeat(base[None, :], pop, axis=0)
+            cand[:, free] = np.clip(rng.normal(mu, sd, (pop, len(free))), lo, hi)
+            pred = self.mean_log10(cand)
+            evals += pop
+            loss = np.mean((pred[:, mask] - t[mask]) ** 2, axis=1)
+            order = np.argsort(loss)
+            k = max(2, int(elite * pop))
+            el = cand[order[:k]][:, free]
+            mu, sd = el.mean(0), np.maximum(el.std(0), 1e-4 * self.x_std[free])
+            if loss[order[0]] < best_loss:
+                best_loss, best = float(loss[order[0]]), cand[order[0]].copy()
+            hist.append(best_loss)
+        out = {"features": best, "loss_network": best_loss, "history": np.array(hist), "network_evals": evals}
+        gate = self.predict(best[None, :])
+        out["gated"] = bool(gate["use_network"][0])
+        if verify_photons > 0:
+            from .batch import from_features
+            fb = best[None, :]
+            if not out["gated"] and cand is not None:  # fallback: the Monte Carlo ranks the last round's best
+                pred = self.mean_log10(cand)
+                loss = np.mean((pred[:, mask] - t[mask]) ** 2, axis=1)
+                fb = np.concatenate([best[None, :], cand[np.argsort(loss)[:refine]]])
+            inst = from_features(fb, photons=verify_photons, seed=seed + 1)
+            r = batch.run(inst)["ring_time"].reshape(len(fb), -1)
+            mc_loss = np.mean((np.log10(r[:, mask] + self.floor) - t[mask]) ** 2, axis=1)
+            j = int(np.argmin(mc_loss))
+            out["features"], out["loss_mc"], out["mc_evals"] = fb[j], float(mc_loss[j]), len(fb)
+        return out
+
     def close(self):
         for m in self.members:
             m.close()

@@ -37,23 +37,6 @@ constexpr int kMaxLayers = 9;
 
 __device__ __forceinline__ float f32(uint32_t r) { return __uint_as_float(r); }
 
-__device__ __forceinline__ void store_bf16x32(bf16* p, const float (&v)[32]) {
-    uint4* q = reinterpret_cast<uint4*>(p);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        __nv_bfloat162 a = __floats2bfloat162_rn(v[8 * j + 0], v[8 * j + 1]);
-        __nv_bfloat162 b = __floats2bfloat162_rn(v[8 * j + 2], v[8 * j + 3]);
-        __nv_bfloat162 c = __floats2bfloat162_rn(v[8 * j + 4], v[8 * j + 5]);
-        __nv_bfloat162 d = __floats2bfloat162_rn(v[8 * j + 6], v[8 * j + 7]);
-        uint4 u;
-        u.x = *reinterpret_cast<uint32_t*>(&a);
-        u.y = *reinterpret_cast<uint32_t*>(&b);
-        u.z = *reinterpret_cast<uint32_t*>(&c);
-        u.w = *reinterpret_cast<uint32_t*>(&d);
-        q[j] = u;
-    }
-}
-
 __device__ __forceinline__ void load_bf16x32(const bf16* p, float (&v)[32]) {
     const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
@@ -70,6 +53,29 @@ __device__ __forceinline__ void load_bf16x32(const bf16* p, float (&v)[32]) {
     }
 }
 
+// The warp's 32 rows x 32 columns (lane t holds row row0 + t) to a row-major matrix through the
+// warp's shared-memory tile: 32 stores, each one row segment of 32 consecutive elements.
+__device__ __forceinline__ void warp_rows_f32(float* sw, const float (&v)[32], float* dst, size_t ld, int row0, int col0,
+                                              int ncols, int lane) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sw[lane * 33 + j] = v[j];
+    __syncwarp();
+    if (col0 + lane < ncols) {
+#pragma unroll 4
+        for (int k = 0; k < 32; ++k) dst[(size_t)(row0 + k) * ld + col0 + lane] = sw[k * 33 + lane];
+    }
+    __syncwarp();
+}
+__device__ __forceinline__ void warp_rows_bf16(float* sw, const float (&v)[32], bf16* dst, size_t ld, int row0, int col0,
+                                               int lane) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sw[lane * 33 + j] = v[j];
+    __syncwarp();
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) dst[(size_t)(row0 + k) * ld + col0 + lane] = __float2bfloat16_rn(sw[k * 33 + lane]);
+    __syncwarp();
+}
+
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = 1.0f / (1.0f + __expf(-z));
@@ -83,11 +89,11 @@ struct EpiF32 {
     float* d;
     int ld;
     size_t split_stride;
-    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int) const {
-        float* p = d + blockIdx.z * split_stride + (size_t)row * ld + col0;
+    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int lane, float* sw) const {
+        float v[32];
 #pragma unroll
-        for (int j = 0; j < 32; j += 4)
-            *reinterpret_cast<float4*>(p + j) = make_float4(f32(r[j]), f32(r[j + 1]), f32(r[j + 2]), f32(r[j + 3]));
+        for (int j = 0; j < 32; ++j) v[j] = f32(r[j]);
+        warp_rows_f32(sw, v, d + blockIdx.z * split_stride, (size_t)ld, row - lane, col0, col0 + 32, lane);
     }
 };
 
@@ -99,14 +105,14 @@ struct EpiHidden {
     bf16* z;    // nullable
     bf16* at;   // nullable, [cols x ldt]
     int ldt;
-    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int) const {
+    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int lane, float* sw) const {
         float v[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) v[j] = f32(r[j]) + __ldg(&bias[col0 + j]);
-        if (z) store_bf16x32(z + (size_t)row * lda + col0, v);
+        if (z) warp_rows_bf16(sw, v, z, (size_t)lda, row - lane, col0, lane);
 #pragma unroll
         for (int j = 0; j < 32; ++j) v[j] = silu(v[j]);
-        store_bf16x32(a + (size_t)row * lda + col0, v);
+        warp_rows_bf16(sw, v, a, (size_t)lda, row - lane, col0, lane);
         if (at) {
 #pragma unroll
             for (int j = 0; j < 32; ++j) at[(size_t)(col0 + j) * ldt + row] = __float2bfloat16_rn(v[j]);
@@ -132,19 +138,11 @@ struct EpiOut {
     const float* colw;  // nullable: per-output weight of the squared error
     float* loss;
     const int* step;
-    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int lane) const {
+    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int lane, float* sw) const {
         float v[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) v[j] = f32(r[j]) + __ldg(&bias[col0 + j]);
-        if (y && col0 < n_out) {
-            float* p = y + (size_t)row * ldy + col0;
-            if (col0 + 32 <= n_out && (ldy % 4) == 0) {
-#pragma unroll
-                for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(p + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-            } else {
-                for (int j = 0; j < 32 && col0 + j < n_out; ++j) p[j] = v[j];
-            }
-        }
+        if (y && col0 < n_out) warp_rows_f32(sw, v, y, (size_t)ldy, row - lane, col0, n_out, lane);
         if (t) {
             float se = 0.0f;
             const float* tp = t + (size_t)row * ldtg;
@@ -156,7 +154,7 @@ struct EpiOut {
                 se = fmaf(wd, d, se);
                 v[j] = wd * scale;
             }
-            store_bf16x32(dy + (size_t)row * lddy + col0, v);
+            warp_rows_bf16(sw, v, dy, (size_t)lddy, row - lane, col0, lane);
 #pragma unroll
             for (int j = 0; j < 32; ++j) dyt[(size_t)(col0 + j) * lddyt + row] = __float2bfloat16_rn(v[j]);
 #pragma unroll
@@ -173,12 +171,12 @@ struct EpiBwd {
     bf16* dz;
     bf16* dzt;
     int ldt;
-    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int) const {
+    __device__ void apply(int row, int col0, const uint32_t (&r)[32], int lane, float* sw) const {
         float zv[32], v[32];
         load_bf16x32(z + (size_t)row * ldz + col0, zv);
 #pragma unroll
         for (int j = 0; j < 32; ++j) v[j] = f32(r[j]) * dsilu(zv[j]);
-        store_bf16x32(dz + (size_t)row * ldz + col0, v);
+        warp_rows_bf16(sw, v, dz, (size_t)ldz, row - lane, col0, lane);
 #pragma unroll
         for (int j = 0; j < 32; ++j) dzt[(size_t)(col0 + j) * ldt + row] = __float2bfloat16_rn(v[j]);
     }

@@ -127,8 +127,9 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
-// Epilogue interface: Epi::apply(row, col0, acc[32]) for tile row `row` (global) and the 32
-// consecutive global columns starting at col0; `lane` for warp-level reductions.
+// Epilogue interface: Epi::apply(row, col0, acc[32], lane, scratch) for tile row `row` (global) and
+// the 32 consecutive global columns starting at col0; `lane` for warp-level work; `scratch` is the
+// warp's 32 x 33 FP32 shared-memory tile (rows of the warp's 32 tile rows, padded).
 template <int BN, class Epi>
 __global__ void __launch_bounds__(128, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int k_blocks_per_split,
@@ -203,12 +204,15 @@ __global__ void __launch_bounds__(128, 1)
     // warp-uniform: tcgen05.ld is a .sync.aligned instruction
     if (__all_sync(0xffffffffu, ok && *((volatile int*)err) == 0)) {
         const int row = m0 + warp * 32 + lane;
+        // the operand ring is idle once `done` has fired: its first 16.5 KB serve as per-warp
+        // 32 x 33 FP32 staging tiles for row-coalesced stores
+        float* scratch = reinterpret_cast<float*>(aligned) + warp * (32 * 33);
 #pragma unroll 1
         for (int c = 0; c < BN; c += 32) {
             uint32_t r[32];
             tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
             tmem_ld_wait();
-            epi.apply(row, n0 + c, r, lane);
+            epi.apply(row, n0 + c, r, lane, scratch);
         }
     }
     tc_fence_before();

@@ -354,7 +354,7 @@ int launch_gemm(const void* a, int rows_a, const void* b, int n, int k, int spli
     st = make_map(&mb, b, (uint64_t)n, (uint64_t)k, BN);
     if (st) return st;
     const dim3 grid(n / BN, rows_a / tc::kBM, splits);
-    tc::gemm_kernel<BN, Epi><<<grid, 128, tc::smem_bytes(BN), stream>>>(ma, mb, k / tc::kBK / splits, err, epi);
+    tc::gemm_kernel<BN, Epi><<<grid, tc::kThreads, tc::smem_bytes(BN), stream>>>(ma, mb, k / tc::kBK / splits, err, epi);
     XM_CUDA(cudaGetLastError());
     return XMC_OK;
 }

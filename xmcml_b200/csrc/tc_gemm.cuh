@@ -2,14 +2,15 @@
 //
 //   D[M x N] = A[M x K] . B[N x K]^T      A, B bf16 row-major (K contiguous), D accumulated in FP32
 //
-// One CTA of 128 threads computes a 128 x BN tile of D over a range of K (split-K when the grid's
+// One CTA of 256 threads computes a 128 x BN tile of D over a range of K (split-K when the grid's
 // z extent is > 1). Operand tiles of 128 (A) and BN (B) rows x 64 bf16 (128 B) are brought into
 // shared memory by TMA (cp.async.bulk.tensor.2d, 128-byte swizzle) through a 2-stage ring of
 // mbarrier-tracked buffers; one thread issues the tcgen05.mma instructions (M = 128, N = BN,
 // K = 16 each, both operands K-major, read from shared memory through matrix descriptors) into a
 // TMEM accumulator of BN columns, and tcgen05.commit signals the ring's "empty" barriers and the
-// final "done" barrier. The four warps then read the accumulator back with tcgen05.ld (warp w owns
-// TMEM lanes 32w..32w+31, i.e. tile rows) and run the epilogue functor on 32 columns at a time.
+// final "done" barrier. The eight warps then read the accumulator back with tcgen05.ld (warp w reads
+// TMEM lanes 32 (w % 4)..+31, i.e. tile rows, and every other 32-column chunk starting at 32 (w / 4))
+// and run the epilogue functor on 32 columns at a time.
 //
 // Every wait on an mbarrier is bounded: after kWaitNs of polling the kernel records an error in
 // *err, stops issuing work, and still releases its TMEM before returning.
@@ -23,6 +24,7 @@ namespace xmc {
 namespace tc {
 
 constexpr int kBM = 128;          // tile rows (MMA M)
+constexpr int kThreads = 256;     // 8 warps: warp w reads TMEM lanes 32 (w % 4).., column half w / 4
 constexpr int kBK = 64;           // K per stage: 64 bf16 = one 128-byte swizzle row
 constexpr int kStages = 2;  // small enough that two CTAs (BN = 256) share an SM: one's epilogue
                               // overlaps the other's loads and MMAs
@@ -131,10 +133,11 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
 // the 32 consecutive global columns starting at col0; `lane` for warp-level work; `scratch` is the
 // warp's 32 x 33 FP32 shared-memory tile (rows of the warp's 32 tile rows, padded).
 template <int BN, class Epi>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kThreads, 2)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int k_blocks_per_split,
                 int* err, const Epi epi) {
     static_assert(BN == 64 || BN == 128 || BN == 256, "BN");
+    static_assert(kStages * stage_bytes(BN) >= (kThreads / 32) * 32 * 33 * 4, "epilogue staging tiles fit the ring");
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-byte aligned stage ring
@@ -203,14 +206,15 @@ __global__ void __launch_bounds__(128, 1)
     tc_fence_after();
     // warp-uniform: tcgen05.ld is a .sync.aligned instruction
     if (__all_sync(0xffffffffu, ok && *((volatile int*)err) == 0)) {
-        const int row = m0 + warp * 32 + lane;
-        // the operand ring is idle once `done` has fired: its first 16.5 KB serve as per-warp
+        const int quarter = warp & 3;  // TMEM lanes (tile rows) this warp may read
+        const int row = m0 + quarter * 32 + lane;
+        // the operand ring is idle once `done` has fired: its first 33 KB serve as per-warp
         // 32 x 33 FP32 staging tiles for row-coalesced stores
         float* scratch = reinterpret_cast<float*>(aligned) + warp * (32 * 33);
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 32) {
+        for (int c = (warp >> 2) * 32; c < BN; c += 64) {
             uint32_t r[32];
-            tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+            tmem_ld32(taddr + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, r);
             tmem_ld_wait();
             epi.apply(row, n0 + c, r, lane, scratch);
         }

@@ -304,7 +304,12 @@ int xmc_cancel(xmc_context* ctx);
 
 int xmc_destroy(xmc_context* ctx);
 
-/* One call = create + run + destroy. */
+/* One call = create + run on a device context. The context of the last model is kept for the next
+ * call when nothing its device image depends on has changed (a 64-bit fingerprint over the layers,
+ * surfaces, detectors, Area, time bins, start, biasing fields, weight tables, caller BVH and options;
+ * numberOfPhotons may change), as the reference's launchers call LaunchOMP repeatedly on one
+ * InputInfo. Calls are serialised by a lock. xmc_launch_release() frees the kept context. */
+int xmc_launch_release(void);
 int xmc_launch(const InputInfo* input, OutputInfo* output, uint64_t seed,
                uint64_t first_photon_id, const xmc_options* opt, xmc_ledger* ledger);
 

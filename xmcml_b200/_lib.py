@@ -83,6 +83,7 @@ def load(path: str | None = None) -> C.CDLL:
         "xmc_mlp_destroy": (C.c_int, [C.c_void_p]),
         "xmc_mlp_set_output_weights": (C.c_int, [C.c_void_p, P(C.c_float)]),
         "xmc_weight_integral_table": (C.c_int, [P(S.InputInfo), C.c_int]),
+        "xmc_launch_release": (C.c_int, []),
         "xmc_gemm_bf16": (C.c_int, [P(C.c_uint16), P(C.c_uint16), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                     P(C.c_float)]),
     }
@@ -115,6 +116,6 @@ EXPORTS = [
     "xmc_batch_get_tuning", "xmc_batch_autotune", "xmc_batch_destroy",
     "xmc_mlp_create", "xmc_mlp_param_count", "xmc_mlp_set_params", "xmc_mlp_get_params", "xmc_mlp_forward",
     "xmc_mlp_forward_timed", "xmc_mlp_gradients", "xmc_mlp_set_dataset", "xmc_mlp_train", "xmc_mlp_destroy",
-    "xmc_mlp_set_output_weights", "xmc_weight_integral_table",
+    "xmc_mlp_set_output_weights", "xmc_weight_integral_table", "xmc_launch_release",
     "xmc_gemm_bf16",
 ]

@@ -5,8 +5,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "xmc_internal.h"
@@ -39,7 +42,7 @@ static void free_context(Context* c) {
                      c->d_big, c->d_cancel, c->d_wtab};
     for (void* p : dbufs)
         if (p) cudaFree(p);
-    void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status};
+    void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status, c->h_maps};
     for (void* p : hbufs)
         if (p) cudaFreeHost(p);
     for (cudaEvent_t& e : c->ev)
@@ -47,6 +50,30 @@ static void free_context(Context* c) {
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->cancel_stream) cudaStreamDestroy(c->cancel_stream);
     delete c;
+}
+
+// dst[i] += src[i] * scale (scale != 0) or dst[i] += src[i] as integers, over n elements on up to 16
+// host threads (the caller's FP64 / u64 output arrays are large: up to detectors x voxels).
+template <typename D>
+static void accumulate(D* dst, const unsigned long long* src, size_t n, double scale) {
+    auto body = [&](size_t a, size_t b) {
+        for (size_t i = a; i < b; ++i) {
+            if constexpr (std::is_same<D, double>::value) dst[i] += (double)src[i] * scale;
+            else dst[i] += src[i];
+        }
+    };
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (n < (size_t)1 << 18 || hw == 1) {
+        body(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t per = (n + hw - 1) / hw;
+    for (unsigned t = 0; t < hw; ++t) {
+        const size_t a = t * per, b = std::min(n, a + per);
+        if (a < b) pool.emplace_back(body, a, b);
+    }
+    for (auto& th : pool) th.join();
 }
 
 // mcml_kernel.cpp:16-37 (FP64, exactly as the reference computes it)
@@ -601,8 +628,7 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         if (out->gridSize != c->grid_size) return fail(XMC_ERR_INVALID_INPUT, "output gridSize does not match the input Area");
         if (out->numberOfDetectors != c->n_dets) return fail(XMC_ERR_INVALID_INPUT, "output numberOfDetectors does not match the input");
         out->specularReflectance = c->rsp;
-        if (out->absorption)
-            for (int i = 0; i < c->grid_size; ++i) out->absorption[i] += (double)c->h_absorb[i] * inv_scale;
+        if (out->absorption) accumulate(out->absorption, c->h_absorb, (size_t)c->grid_size, inv_scale);
         for (int d = 0; d < c->n_dets; ++d) {
             DetectorInfo& D = out->detectorInfo[d];
             const unsigned long long* t = c->h_det + 4 * (size_t)d;
@@ -626,26 +652,39 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         led->h2d_bytes = c->h2d_bytes + sizeof(KParams);
         led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16;
     }
-    if (out && scat && out->scattering) {
-        std::vector<unsigned long long> m((size_t)c->grid_size);
-        XMC_CUDA(cudaMemcpy(m.data(), c->d_scatter, absorb_b, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < c->grid_size; ++i) out->scattering[i] += (double)m[i] * inv_scale;
+    // maps: one pinned staging buffer (kept by the context) for the scattering map and every
+    // detector's trajectory map, one copy each, then the additions into the caller's arrays
+    const bool want_scat = out && scat && out->scattering;
+    const bool want_traj = out && traj;
+    if (want_scat || want_traj) {
+        const size_t need = absorb_b * ((want_scat ? 1 : 0) + (want_traj ? (size_t)std::max(1, c->n_dets) : 0));
+        if (c->h_maps_bytes < need) {
+            if (c->h_maps) cudaFreeHost(c->h_maps);
+            c->h_maps = nullptr;
+            c->h_maps_bytes = 0;
+            XMC_CUDA(cudaHostAlloc((void**)&c->h_maps, need, cudaHostAllocDefault));
+            c->h_maps_bytes = need;
+        }
+        unsigned long long* hs = c->h_maps;
+        unsigned long long* ht = c->h_maps + (want_scat ? (size_t)c->grid_size : 0);
+        if (want_scat) XMC_CUDA(cudaMemcpyAsync(hs, c->d_scatter, absorb_b, cudaMemcpyDeviceToHost, c->stream));
+        if (want_traj)
+            XMC_CUDA(cudaMemcpyAsync(ht, c->d_traj, absorb_b * (size_t)std::max(1, c->n_dets), cudaMemcpyDeviceToHost,
+                                     c->stream));
+        XMC_CUDA(cudaStreamSynchronize(c->stream));
+        if (want_scat) accumulate(out->scattering, hs, (size_t)c->grid_size, inv_scale);
+        if (want_traj)
+            for (int d = 0; d < c->n_dets; ++d) {
+                DetectorInfo& D = out->detectorInfo[d];
+                if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
+                accumulate(D.trajectory, ht + (size_t)d * c->grid_size, (size_t)c->grid_size, 0.0);
+            }
     }
     unsigned long long mismatch = 0;
     if (traj) {
         unsigned long long rl[kLedgerSlots];
         XMC_CUDA(cudaMemcpy(rl, c->d_replay_ledger, led_b, cudaMemcpyDeviceToHost));
         mismatch = rl[L_N_REPLAY_MISMATCH];
-        if (out) {
-            std::vector<unsigned long long> m((size_t)c->grid_size);
-            for (int d = 0; d < c->n_dets; ++d) {
-                DetectorInfo& D = out->detectorInfo[d];
-                if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
-                XMC_CUDA(cudaMemcpy(m.data(), (unsigned long long*)c->d_traj + (size_t)d * c->grid_size, absorb_b,
-                                    cudaMemcpyDeviceToHost));
-                for (int i = 0; i < c->grid_size; ++i) D.trajectory[i] += m[i];
-            }
-        }
     }
     if (led) led->n_replay_mismatch = mismatch;
     if (c->h_status[0] & 2) return fail(XMC_ERR_CANCELLED, "run cancelled");
@@ -750,16 +789,118 @@ int xmc_destroy(xmc_context* ctx) {
     return XMC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// 64-bit fingerprint of everything a device image depends on (word-wise multiply-xorshift mix).
+struct Fingerprint {
+    uint64_t h = 0x9E3779B97F4A7C15ull;
+    void add(const void* p, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        if (!b) n = 0;
+        size_t i = 0;
+        for (; i + 8 <= n; i += 8) {
+            uint64_t w;
+            std::memcpy(&w, b + i, 8);
+            mix(w);
+        }
+        uint64_t w = 0;
+        std::memcpy(&w, b + i, n - i);
+        mix(w ^ ((uint64_t)n << 56));
+    }
+    template <typename T> void val(const T& v) { add(&v, sizeof(v)); }
+    void mix(uint64_t w) {
+        h ^= w;
+        h *= 0xff51afd7ed558ccdull;
+        h ^= h >> 32;
+    }
+};
+
+uint64_t input_fingerprint(const InputInfo* in, const xmc_options* opt) {
+    Fingerprint f;
+    f.val(in->numberOfLayers); f.val(in->numberOfSurfaces); f.val(in->numberOfCubeDetectors);
+    f.val(in->numberOfRingDetectors); f.val(in->minWeight); f.val(in->timeStart); f.val(in->timeFinish);
+    f.val(in->timeScaleSize); f.val(in->startPosition); f.val(in->startDirection); f.val(in->useBiasing);
+    f.val(in->weightIntegralPrecision); f.val(in->weightTablePrecision); f.val(in->attractiveFactor);
+    f.val(in->targetPoint); f.add(in->targetRangeLayers, sizeof(in->targetRangeLayers));
+    if (in->area) f.val(*in->area);
+    for (int l = 0; in->layerInfo && l < in->numberOfLayers; ++l) {
+        const LayerInfo& L = in->layerInfo[l];
+        f.val(L.refractiveIndex); f.val(L.absorptionCoefficient); f.val(L.scatteringCoefficient); f.val(L.anisotropy);
+        f.val(L.numberOfSurfaces);
+        f.add(L.surfaceId, sizeof(int) * (size_t)std::max(0, L.numberOfSurfaces));
+    }
+    for (int s = 0; in->surface && s < in->numberOfSurfaces; ++s) {
+        const Surface& S = in->surface[s];
+        f.val(S.numberOfVertices); f.val(S.numberOfTriangles);
+        f.add(S.vertices, sizeof(double3) * (size_t)std::max(0, S.numberOfVertices));
+        f.add(S.triangles, sizeof(int3) * (size_t)std::max(0, S.numberOfTriangles));
+    }
+    f.add(in->cubeDetector, sizeof(CubeDetector) * (size_t)std::max(0, in->numberOfCubeDetectors));
+    f.add(in->ringDetector, sizeof(RingDetector) * (size_t)std::max(0, in->numberOfRingDetectors));
+    f.val(in->numberOfWeightTables);
+    for (int k = 0; in->weightTable && k < in->numberOfWeightTables; ++k) {
+        const WeightIntegralTable& T = in->weightTable[k];
+        f.val(T.anisotropy); f.val(T.numberOfElements);
+        f.add(T.elements, sizeof(double) * (size_t)std::max(0, T.numberOfElements));
+    }
+    if (in->bvhTree) {
+        const BVHTree& B = *in->bvhTree;
+        f.val(B.numOfNodes); f.val(B.root); f.val(B.numOfTriangles);
+        f.add(B.nodes, sizeof(BVHNode) * (size_t)std::max(0, B.numOfNodes));
+        f.add(B.triangles, sizeof(Triangle) * (size_t)std::max(0, B.numOfTriangles));
+    } else {
+        f.val((uint64_t)0);
+    }
+    xmc_options o;
+    xmc_default_options(&o);
+    if (opt && opt->struct_size) std::memcpy(&o, opt, std::min((size_t)opt->struct_size, sizeof(o)));
+    o.struct_size = sizeof(o);
+    f.val(o);
+    return f.h;
+}
+
+// The device context of the last model run through xmc_launch, kept for the next call on the same
+// model contents (the reference's launchers call LaunchOMP repeatedly on one InputInfo).
+std::mutex g_launch_mutex;
+xmc::Context* g_launch_ctx = nullptr;
+uint64_t g_launch_fp = 0;
+
+}  // namespace
+
+extern "C" {
+
 int xmc_launch(const InputInfo* input, OutputInfo* output, uint64_t seed, uint64_t first_photon_id,
                const xmc_options* opt, xmc_ledger* ledger) {
-    xmc_context* c = nullptr;
-    int st = xmc_create(input, opt, &c);
-    if (st) return st;
-    st = xmc_run(c, seed, first_photon_id, input->numberOfPhotons, output, ledger);
-    std::string keep = g_last_error;
-    xmc_destroy(c);
-    set_error(keep);
+    if (!input) return fail(XMC_ERR_INVALID_INPUT, "input is NULL");
+    std::lock_guard<std::mutex> lock(g_launch_mutex);
+    const uint64_t fp = input_fingerprint(input, opt);
+    if (!g_launch_ctx || fp != g_launch_fp) {
+        if (g_launch_ctx) free_context(g_launch_ctx);
+        g_launch_ctx = nullptr;
+        xmc_context* c = nullptr;
+        int st = xmc_create(input, opt, &c);
+        if (st) return st;
+        g_launch_ctx = reinterpret_cast<Context*>(c);
+        g_launch_fp = fp;
+    }
+    int st = xmc_run(reinterpret_cast<xmc_context*>(g_launch_ctx), seed, first_photon_id, input->numberOfPhotons, output,
+                     ledger);
+    if (st && st != XMC_ERR_BUDGET && st != XMC_ERR_CANCELLED) {  // a failed run: do not keep its context
+        std::string keep = g_last_error;
+        free_context(g_launch_ctx);
+        g_launch_ctx = nullptr;
+        set_error(keep);
+    }
     return st;
+}
+
+int xmc_launch_release(void) {
+    std::lock_guard<std::mutex> lock(g_launch_mutex);
+    if (g_launch_ctx) free_context(g_launch_ctx);
+    g_launch_ctx = nullptr;
+    return XMC_OK;
 }
 
 int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* rng, int numThreads) {

@@ -179,6 +179,8 @@ struct Context {
     // pinned read-back buffers
     unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;
     unsigned long long* h_tbin = nullptr; unsigned long long* h_ledger = nullptr;
+    unsigned long long* h_maps = nullptr;   // pinned staging of the scattering and trajectory maps (lazy)
+    size_t h_maps_bytes = 0;
     int* h_status = nullptr;
     uint64_t last_n = 0;
     double last_kernel_ms = 0.0, last_total_ms = 0.0;

@@ -415,3 +415,39 @@ def test_biasing_matches_oracle(tmp_path, factor):
     assert np.all(np.abs(zt) < 3.0)
     for k in ("bias_gained", "bias_lost"):
         assert led[k] == pytest.approx(oled[k] / n, rel=0.05)
+
+
+def test_launch_keeps_context_only_for_unchanged_models(tmp_path):
+    """xmc_launch_omp keeps the device image of the last model: a second call on the unchanged model
+    repeats a fresh run bit for bit, and after a change of an optical property the result is the new
+    model's (as a fresh context gives it), not the kept image's."""
+    n = 20_000
+    xml, surf = scenes.planar(photons=n).write(str(tmp_path), "cache")
+    m = api.Model(xml, surf)
+
+    def via_launch(key):
+        out = api.Output(m)
+        g = S.MCG59()
+        g.value, g.offset = key, 1
+        api.launch_omp(m, out, g, 0)
+        return out.detector_weights(), out.absorption.copy()
+
+    def fresh(key):
+        out = api.Output(m)
+        t = api.Transport(m, scattering=True, trajectories=True)
+        t.run(n, seed=key, output=out)
+        t.close()
+        return out.detector_weights(), out.absorption.copy()
+
+    _lib.check(_lib.load().xmc_launch_release())
+    a1 = via_launch(99)
+    a2 = via_launch(99)  # kept context
+    assert np.array_equal(a1[0], a2[0]) and np.array_equal(a1[1], a2[1])
+    f = fresh(99)
+    assert np.array_equal(a1[0], f[0]) and np.array_equal(a1[1], f[1])
+    m.info.layerInfo[1].scatteringCoefficient *= 1.5
+    b = via_launch(99)
+    fb = fresh(99)
+    assert np.array_equal(b[0], fb[0]) and np.array_equal(b[1], fb[1])
+    assert not np.array_equal(b[0], a1[0])
+    _lib.check(_lib.load().xmc_launch_release())

@@ -211,7 +211,8 @@ typedef enum xmc_status {
                                           the ledger's absorbed_outside term                         */
 #define XMC_SCATTERING_MAP  (1u << 2)  /* tally the z-plane crossing map OutputInfo.scattering         */
 #define XMC_DETECTOR_TRAJ   (1u << 3)  /* tally per-detector trajectory maps DetectorInfo.trajectory
-                                          (a second, replay pass over the detected photons)         */
+                                          (from a per-thread crossing log; photons whose log overflows
+                                          are walked again in a replay pass)                        */
 #define XMC_LARGE_GRID      (1u << 4)  /* accept Area partitions above 256 per axis (the reference wraps
                                           voxel indices at 256; this library indexes them in full)    */
 
@@ -226,7 +227,10 @@ typedef struct xmc_options {
     int32_t  blocks_per_sm;        /* resident blocks per SM (0 = occupancy maximum)              */
     int32_t  photons_per_chunk;    /* photon ids a warp claims at a time (0 = 64)                 */
     int32_t  smem_nodes;           /* BVH nodes staged in shared memory (-1 = none, 0 = auto)      */
-    int32_t  reserved[7];
+    int32_t  trajectory_log;       /* XMC_DETECTOR_TRAJ: z-plane crossings logged per resident thread
+                                    * (0 = 1024, at most 65536; -1 = no log, every detected photon
+                                    * is replayed)                                                 */
+    int32_t  reserved[6];
 } xmc_options;
 
 /* Energy ledger of one or more runs: every photon's start weight 1 is split exactly into these
@@ -259,6 +263,8 @@ typedef struct xmc_ledger {
     uint64_t bias_gained_fx;       /* biasing: weight added by the weight-table factor W / p > 1  */
     uint64_t bias_lost_fx;         /* biasing: weight removed by factors < 1                      */
     double bias_gained, bias_lost; /* the same per launched photon                               */
+    uint64_t n_trajectory_replayed;/* XMC_DETECTOR_TRAJ: detected photons walked again because their
+                                    * crossing log overflowed                                       */
 } xmc_ledger;
 
 typedef struct xmc_context xmc_context;

@@ -199,21 +199,30 @@ def test_split_runs_add_up(tmp_path):
     t.close()
 
 
-@pytest.mark.parametrize("which", ["planar", "heightfield"])
-def test_scattering_and_trajectory_maps(tmp_path, which):
+@pytest.mark.parametrize("which,log", [("planar", 0), ("heightfield", 0), ("heightfield", 16), ("planar", -1)])
+def test_scattering_and_trajectory_maps(tmp_path, which, log):
     """UpdatePhotonTrajectory / UpdateDetectorTrajectory (mcml_kernel.cpp:750-810): the scattering map
     (weight at every z-plane crossing through voxel centres) and, per detector, the crossing counts
-    of the photons it detected (GPU: replay pass over the detected photons)."""
+    of the photons it detected. GPU: each thread's crossing log (log = 0: 1024 entries), counted at
+    detection; a photon whose log overflows (log = 16: most of them) or every detected photon (log =
+    -1: no log) is walked again by the replay pass."""
     n = 50_000
     sc = scenes.planar(photons=n) if which == "planar" else scenes.height_field_tissue(photons=n, grid=64, time_bins=10)
     xml, surf = sc.write(str(tmp_path), "maps_" + which)
     m = api.Model(xml, surf)
-    t = api.Transport(m, roulette=True, scattering=True, trajectories=True)
+    t = api.Transport(m, roulette=True, scattering=True, trajectories=True, trajectory_log=log)
     led = t.run(n, seed=31)
     maps = t.maps()
     tal = t.tallies()
     t.close()
     assert led["n_replay_mismatch"] == 0
+    n_det = int(tal["det_count"].sum())
+    if log == -1:
+        assert led["n_trajectory_replayed"] == n_det
+    elif log == 16:
+        assert 0 < led["n_trajectory_replayed"] < n_det
+    else:
+        assert led["n_trajectory_replayed"] < 0.01 * n_det
     out = api.Output(m)
     opts = oracle_opts_for(roulette=True)
     opts.flags |= B.OFLAG_SCATTERING | B.OFLAG_TRAJECTORY
@@ -234,8 +243,31 @@ def test_scattering_and_trajectory_maps(tmp_path, which):
     sel = ot > 1000
     print(which, "trajectory totals (first 5)", gt[:5], ot[:5])
     assert np.all(np.abs(gt - ot)[sel] / ot[sel] < 0.03)
-    # every detected photon was replayed: detector counts of the run pass equal those of the oracle
+    # the detectors that saw photons are the oracle's
     assert np.array_equal(tal["det_count"][:D] > 0, out.detector_counts() > 0)
+
+
+def test_trajectory_log_equals_replay(tmp_path):
+    """The crossing log and the replay pass count the same crossings of the same photons (same
+    counter-RNG draws): the integer trajectory and scattering maps agree exactly whether every
+    detected photon, some (a log that overflows) or almost none is replayed."""
+    n = 40_000
+    sc = scenes.height_field_tissue(photons=n, grid=64, time_bins=10)
+    xml, surf = sc.write(str(tmp_path), "maps_log")
+    m = api.Model(xml, surf)
+    res = {}
+    for log in (-1, 16, 0):
+        t = api.Transport(m, roulette=True, scattering=True, trajectories=True, trajectory_log=log)
+        led = t.run(n, seed=8)
+        res[log] = (t.maps(), t.tallies()["det_count"], led["n_trajectory_replayed"])
+        t.close()
+    base_maps, base_det, _ = res[-1]
+    assert res[16][2] > 0 and res[0][2] < res[16][2]
+    for log in (16, 0):
+        maps, det, _ = res[log]
+        assert np.array_equal(det, base_det)
+        assert np.array_equal(maps["scattering"], base_maps["scattering"])
+        assert np.array_equal(maps["trajectory"], base_maps["trajectory"])
 
 
 def test_launch_omp_shim_accumulates(tmp_path):

@@ -39,7 +39,7 @@ static void free_context(Context* c) {
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
                      c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
                      c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_z, c->d_cell_entries,
-                     c->d_big, c->d_cancel, c->d_wtab};
+                     c->d_big, c->d_cancel, c->d_wtab, c->d_xlog};
     for (void* p : dbufs)
         if (p) cudaFree(p);
     void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status, c->h_maps};
@@ -138,6 +138,8 @@ static int validate(const InputInfo* in, const xmc_options& opt) {
     }
     if (!(opt.roulette_chance > 0 && opt.roulette_chance <= 1)) return fail(XMC_ERR_INVALID_INPUT, "roulette_chance must be in (0, 1]");
     if (opt.beam_radius < 0) return fail(XMC_ERR_INVALID_INPUT, "beam_radius must be >= 0");
+    if (opt.trajectory_log < -1 || opt.trajectory_log > 65536)
+        return fail(XMC_ERR_RANGE, "trajectory_log must be -1, 0 or at most 65536");
     return XMC_OK;
 }
 
@@ -533,6 +535,13 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     if (occ <= 0) return bail(fail(XMC_ERR_DEVICE, "transport kernel cannot be resident with this block size / shared memory"));
     c->blocks_per_sm = opt.blocks_per_sm > 0 ? std::min(opt.blocks_per_sm, occ) : occ;
     c->grid = c->num_sms * c->blocks_per_sm;
+    if ((opt.flags & XMC_DETECTOR_TRAJ) && opt.trajectory_log >= 0) {
+        // crossing log: one row per resident thread, reused photon after photon
+        const unsigned cap = opt.trajectory_log > 0 ? (unsigned)opt.trajectory_log : 1024u;
+        CK(cudaMalloc(&c->d_xlog, sizeof(unsigned) * (size_t)c->grid * c->block * cap));
+        kp.xlog = (unsigned*)c->d_xlog;
+        kp.xlog_cap = cap;
+    }
     CK(cudaStreamSynchronize(c->stream));
 #undef CK
     *out = c;
@@ -568,11 +577,12 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     XMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
     if (n > 0 && !traj) XMC_CUDA(enqueue_transport(c));
     if (n > 0 && traj) {
-        // Detector trajectory maps in two passes per portion of photons: the run pass lists every
-        // detected photon as (index, detector); the replay pass walks exactly those photons again
-        // (same counter-RNG draws, same code) and counts their z-plane crossings in that
-        // detector's map. The reference keeps a per-photon crossing log instead
-        // (PhotonTrajectory, mcml_kernel_types.h:118-124).
+        // Detector trajectory maps: the run pass logs each photon's z-plane crossings per thread
+        // (as the reference's PhotonTrajectory, mcml_kernel_types.h:118-124) and counts the log of
+        // a detected photon in its detector's map. A detected photon whose log overflowed is listed
+        // as (index, detector); the replay pass walks exactly those photons again (same
+        // counter-RNG draws, same code) and counts their crossings in that detector's map.
+        c->last_replayed = 0;
         const uint64_t portion_max = 1ull << 26;
         const uint64_t cap = std::min<uint64_t>(n, portion_max);
         if (c->replay_cap < cap) {
@@ -596,6 +606,7 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
             unsigned long long listed = 0;
             XMC_CUDA(cudaMemcpyAsync(&listed, c->d_replay_count, sizeof(listed), cudaMemcpyDeviceToHost, c->stream));
             XMC_CUDA(cudaStreamSynchronize(c->stream));
+            c->last_replayed += listed;
             kp.mode = 1;
             kp.n_photons = std::min<unsigned long long>(listed, c->replay_cap);
             kp.ledger = (unsigned long long*)c->d_replay_ledger;
@@ -686,7 +697,10 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         XMC_CUDA(cudaMemcpy(rl, c->d_replay_ledger, led_b, cudaMemcpyDeviceToHost));
         mismatch = rl[L_N_REPLAY_MISMATCH];
     }
-    if (led) led->n_replay_mismatch = mismatch;
+    if (led) {
+        led->n_replay_mismatch = mismatch;
+        led->n_trajectory_replayed = traj ? c->last_replayed : 0;
+    }
     if (c->h_status[0] & 2) return fail(XMC_ERR_CANCELLED, "run cancelled");
     if (c->h_status[0] & 1) return fail(XMC_ERR_BUDGET, "a photon reached the step budget and was terminated");
     return XMC_OK;

@@ -165,11 +165,18 @@ __device__ void tally_detection(const KParams& P, const SmemTally& S, const Ph& 
 
 // UpdatePhotonTrajectory (mcml_kernel.cpp:750-792): for a move from p0 to p1, every z-plane through
 // voxel centres between them (inside Area) is crossed at one voxel. The run pass adds the photon's
-// weight to the scattering map there; the replay pass counts the crossing in the trajectory map of
-// the detector the photon reaches (UpdateDetectorTrajectory, :794-810), which the reference does by
-// replaying a per-photon crossing log at detection.
+// weight to the scattering map there and appends the voxel to the thread's crossing log (`xl`, `xn`
+// entries so far, counted past the capacity so that an overflow shows); at detection the log is
+// counted in the detector's trajectory map (UpdateDetectorTrajectory, :794-810, which walks the
+// reference's per-photon PhotonTrajectory the same way). The replay pass, for photons whose log
+// overflowed, counts each crossing in the map of the detector the photon reached.
+// Row of the crossing log of thread `thread` of this block.
+__device__ __forceinline__ unsigned* xlog_row(const KParams& P, unsigned thread) {
+    return P.xlog + ((size_t)blockIdx.x * blockDim.x + thread) * P.xlog_cap;
+}
+
 __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, float x1, float y1, float z1,
-                             unsigned long long w, int rdet) {
+                             unsigned long long w, int rdet, unsigned* __restrict__ xl, unsigned& xn) {
     if (z1 == z0) return;
     float sx = x0, sy = y0, sz = z0, fz = z1, ex = x1 - x0, ey = y1 - y0, ez = z1 - z0;
     if (z1 < z0) {
@@ -185,7 +192,11 @@ __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, flo
         const int idx = area_index(P, fmaf(ex, t, sx), fmaf(ey, t, sy), plane, 0.0f);
         if (idx < 0) break;
         if (P.mode == 0) {
-            if (w) atomicAdd(&P.scatter[idx], (unsigned long long)w);
+            if (w && P.scatter) atomicAdd(&P.scatter[idx], (unsigned long long)w);
+            if (xl) {
+                if (xn < P.xlog_cap) xl[xn] = (unsigned)idx;
+                xn += xn <= P.xlog_cap;  // saturates at capacity + 1: overflowed
+            }
         } else {
             atomicAdd(&P.traj[(size_t)rdet * P.grid + idx], 1ull);
         }
@@ -279,7 +290,8 @@ __device__ __forceinline__ void biased_spin(const KParams& P, const DevLayer& L,
 
 }  // namespace
 
-template <bool kBias>
+// kBias: biased spin with 64-bit weights; kLog: run pass that logs crossings for the trajectory maps
+template <bool kBias, bool kLog>
 __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     using WT = typename std::conditional<kBias, unsigned long long, uint32_t>::type;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -312,18 +324,41 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     const unsigned lt_mask = (1u << lane) - 1u;
     const bool area_kill = !(P.flags & XMC_NO_AREA_KILL);
     const bool roulette = (P.flags & XMC_ROULETTE) != 0;
-    const bool record_planes = P.mode == 1 || (P.flags & XMC_SCATTERING_MAP) != 0;
+    // trajectory maps from the crossing log: each thread's log holds its current photon's crossings
+    const bool log_traj = kLog;
+    const bool record_planes = P.mode == 1 || (P.flags & XMC_SCATTERING_MAP) != 0 || log_traj;
+    unsigned xn = 0;  // crossings of the current photon (capacity + 1: the log overflowed)
 
     unsigned long long cbeg = 0, cend = 0;  // warp-uniform chunk of photon indices
     bool exhausted = false;                 // warp-uniform
     bool alive = false;
     Photon<WT> ph;
+    ph.rdet = -1;
     unsigned steps = 0, retests = 0, n_visit = 0, n_tri = 0;
     unsigned long long bias_gained = 0, bias_lost = 0;
     unsigned long long absorbed = 0, absorbed_out = 0, absorbed_tgt = 0;  // per-thread sums, flushed at the end
     unsigned budget_hit = 0;
 
     for (;;) {
+        // ---- trajectory maps of the photons detected in the last iteration: the whole warp reads
+        // each detected photon's log (coalesced) and counts it in its detector's map ----
+        // (in the run pass a dead photon's rdet holds the detector its log goes to, -1 if none)
+        if (log_traj) {
+            unsigned fl = __ballot_sync(FULL, ph.rdet >= 0);
+            if (fl) {
+                __syncwarp();  // orders each lane's log stores before the other lanes' loads
+                do {
+                    const int src = __ffs(fl) - 1;
+                    fl &= fl - 1u;
+                    const int d = __shfl_sync(FULL, ph.rdet, src);
+                    const unsigned n = __shfl_sync(FULL, xn, src);
+                    const unsigned* xs = xlog_row(P, (threadIdx.x & ~31u) + src);
+                    unsigned long long* tm = P.traj + (size_t)d * P.grid;
+                    for (unsigned j = lane; j < n; j += 32) atomicAdd(&tm[xs[j]], 1ull);
+                } while (fl);
+                ph.rdet = -1;
+            }
+        }
         // ---- refill dead lanes with new photons (warp-level compaction) ----
         unsigned need = __ballot_sync(FULL, !alive && !exhausted);
         while (need) {
@@ -351,6 +386,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             if (((need >> lane) & 1u) && rank < take) {
                 unsigned long long idx = cbeg + rank;
                 ph.rdet = -1;
+                xn = 0;
                 if (P.mode == 1) {
                     const unsigned long long e = P.replay_list[idx];
                     idx = e >> 16;
@@ -413,7 +449,8 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
         ph.px = fmaf(step, ph.dx, ph.px);
         ph.py = fmaf(step, ph.dy, ph.py);
         ph.pz = fmaf(step, ph.dz, ph.pz);
-        if (record_planes) cross_planes(P, ox, oy, oz, ph.px, ph.py, ph.pz, ph.w, ph.rdet);
+        if (record_planes) cross_planes(P, ox, oy, oz, ph.px, ph.py, ph.pz, ph.w, ph.rdet,
+                                        log_traj ? xlog_row(P, threadIdx.x) : nullptr, xn);
         ph.time = fmaf(step, L.n, ph.time);
         if (!(ph.pz > ph.gap_lo && ph.pz < ph.gap_hi)) find_gap(s_zlo, s_zhi, P.n_zocc, ph.pz, ph.gap_lo, ph.gap_hi);
         if ((P.target_mask >> ph.layer) & 1u) ph.trange += step;
@@ -452,7 +489,9 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                     if (P.mode == 0) {
                         if (det >= 0) {
                             tally_detection(P, S, ph, det);
-                            if (P.flags & XMC_DETECTOR_TRAJ) {
+                            if (log_traj && xn <= P.xlog_cap) {
+                                ph.rdet = det;  // the warp counts the log at the top of the next iteration
+                            } else if (P.flags & XMC_DETECTOR_TRAJ) {
                                 const unsigned long long slot = atomicAdd(P.replay_count, 1ull);
                                 if (slot < P.replay_cap)
                                     P.replay_list[slot] = ((ph.pid - P.first_id) << 16) | (unsigned long long)det;
@@ -547,29 +586,41 @@ __global__ void philox_probe_kernel(uint32_t k0, uint32_t k1, unsigned long long
 }
 
 cudaError_t enqueue_transport(Context* ctx) {
-    if (ctx->kp.use_bias)
-        transport_kernel<true><<<ctx->grid, ctx->block, ctx->smem_bytes, ctx->stream>>>(ctx->kp);
-    else
-        transport_kernel<false><<<ctx->grid, ctx->block, ctx->smem_bytes, ctx->stream>>>(ctx->kp);
+    const KParams& kp = ctx->kp;
+    const bool log = kp.mode == 0 && (kp.flags & XMC_DETECTOR_TRAJ) && kp.xlog && kp.xlog_cap > 0;
+    const dim3 g(ctx->grid), b(ctx->block);
+    if (kp.use_bias) {
+        if (log) transport_kernel<true, true><<<g, b, ctx->smem_bytes, ctx->stream>>>(kp);
+        else transport_kernel<true, false><<<g, b, ctx->smem_bytes, ctx->stream>>>(kp);
+    } else {
+        if (log) transport_kernel<false, true><<<g, b, ctx->smem_bytes, ctx->stream>>>(kp);
+        else transport_kernel<false, false><<<g, b, ctx->smem_bytes, ctx->stream>>>(kp);
+    }
     return cudaGetLastError();
 }
 
-template <bool kBias>
+template <bool kBias, bool kLog>
 static cudaError_t occupancy_of(int block, size_t smem, int* blocks_per_sm) {
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, transport_kernel<kBias>);
+    cudaError_t e = cudaFuncGetAttributes(&fa, transport_kernel<kBias, kLog>);
     if (e != cudaSuccess) return e;
     if (block > fa.maxThreadsPerBlock) {
         *blocks_per_sm = 0;
         return cudaSuccess;
     }
-    e = cudaFuncSetAttribute(transport_kernel<kBias>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(transport_kernel<kBias, kLog>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<kBias>, block, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<kBias, kLog>, block, smem);
 }
 
+// Resident blocks per SM of both variants (with and without the crossing log) of the kernel; sets
+// their dynamic shared-memory limit.
 cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm, bool bias) {
-    return bias ? occupancy_of<true>(block, smem, blocks_per_sm) : occupancy_of<false>(block, smem, blocks_per_sm);
+    int a = 0, b = 0;
+    cudaError_t e = bias ? occupancy_of<true, false>(block, smem, &a) : occupancy_of<false, false>(block, smem, &a);
+    if (e == cudaSuccess) e = bias ? occupancy_of<true, true>(block, smem, &b) : occupancy_of<false, true>(block, smem, &b);
+    *blocks_per_sm = a < b ? a : b;
+    return e;
 }
 
 cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n, uint32_t* host_out) {

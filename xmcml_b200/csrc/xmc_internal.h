@@ -131,8 +131,11 @@ struct KParams {
     int grid;                 // nx * ny * nz
     int mode;                 // 0: transport run, 1: trajectory replay of detected photons
     unsigned long long* scatter;        // [grid] scattering map (XMC_SCATTERING_MAP), weight fixed point
-    unsigned long long* traj;           // [n_dets * grid] detector trajectory maps (replay pass), counts
-    unsigned long long* replay_list;    // run: (index << 16 | detector) of detected photons; replay: input
+    unsigned long long* traj;           // [n_dets * grid] detector trajectory maps, counts
+    unsigned* xlog;                     // run: [grid threads][xlog_cap] voxel of each z-plane crossing of the
+    unsigned xlog_cap;                  //      thread's current photon (null / 0: no log, replay every photon)
+    unsigned long long* replay_list;    // run: (index << 16 | detector) of detected photons whose log
+                                        //      overflowed; replay: input
     unsigned long long* replay_count;   // run: number of entries written
     unsigned long long replay_cap;      // run: capacity of replay_list
     // tallies (device, fixed point)
@@ -174,7 +177,9 @@ struct Context {
     cudaStream_t cancel_stream = nullptr;
     void* d_scatter = nullptr; void* d_traj = nullptr; void* d_replay = nullptr; void* d_replay_count = nullptr;
     void* d_replay_ledger = nullptr;
+    void* d_xlog = nullptr;     // crossing log of the trajectory maps
     unsigned long long replay_cap = 0;
+    unsigned long long last_replayed = 0;  // photons the last run walked again (crossing log overflow)
     int* h_cancel = nullptr;  // pinned source of the value xmc_cancel writes into d_cancel
     // pinned read-back buffers
     unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;

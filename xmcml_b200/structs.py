@@ -123,7 +123,7 @@ class XmcOptions(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("flags", C.c_uint32), ("roulette_chance", C.c_double),
                 ("beam_radius", C.c_double), ("max_steps_per_photon", C.c_uint64), ("device", C.c_int32),
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("photons_per_chunk", C.c_int32),
-                ("smem_nodes", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("smem_nodes", C.c_int32), ("trajectory_log", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 _LEDGER_COUNTS = ["photons_launched", "photons_terminated", "steps", "n_escaped_top", "n_escaped_bottom",
@@ -140,7 +140,7 @@ class XmcLedger(C.Structure):
                 + [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_uint64),
                    ("d2h_bytes", C.c_uint64), ("absorbed_target_fx", C.c_uint64), ("absorbed_target", C.c_double),
                    ("bias_gained_fx", C.c_uint64), ("bias_lost_fx", C.c_uint64), ("bias_gained", C.c_double),
-                   ("bias_lost", C.c_double)])
+                   ("bias_lost", C.c_double), ("n_trajectory_replayed", C.c_uint64)])
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

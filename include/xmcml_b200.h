@@ -521,7 +521,9 @@ typedef struct xmc_mlp_spec {
     int32_t n_out;          /* outputs, 1..4096                               */
     int32_t max_rows;       /* row capacity of a forward or training batch    */
     int32_t device;
-    int32_t reserved[9];
+    int32_t forward_kernel; /* inference forward: 0 = one fused kernel for all layers when
+                             * n_out % 4 == 0 (else per layer), 1 = one GEMM per layer  */
+    int32_t reserved[8];
 } xmc_mlp_spec;
 
 typedef struct xmc_mlp xmc_mlp;

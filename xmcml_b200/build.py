@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libxmcml_b200.so")
 
 SOURCES = ["transport.cu", "batch.cu", "surrogate.cu", "weight_table.cu", "noalloc.cu", "capi.cpp", "io.cpp", "bvh.cpp"]
-HEADERS = ["xmc_internal.h", "geom.cuh", "photon.cuh", "tc_gemm.cuh"]
+HEADERS = ["xmc_internal.h", "geom.cuh", "photon.cuh", "tc_gemm.cuh", "mlp_fused.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

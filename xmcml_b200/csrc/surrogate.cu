@@ -23,6 +23,7 @@
 
 #include <cudaTypedefs.h>
 
+#include "mlp_fused.cuh"
 #include "photon.cuh"
 #include "tc_gemm.cuh"
 #include "xmc_internal.h"
@@ -331,6 +332,23 @@ int make_map(CUtensorMap* map, const void* ptr, uint64_t rows, uint64_t cols, ui
     return XMC_OK;
 }
 
+// Tensor map of the FP32 output [rows x n_out] stored in 32 x 32 boxes with the 128-byte swizzle
+// (the fused forward's staging layout); columns past n_out are clipped by the store.
+int make_out_map(CUtensorMap* map, float* y, uint64_t rows, uint64_t n_out) {
+    int st = get_encoder();
+    if (st) return st;
+    if ((reinterpret_cast<uintptr_t>(y) & 15) || (n_out * 4) % 16)
+        return mfail(XMC_ERR_INVALID_INPUT, "tensor map: misaligned output");
+    const cuuint64_t dims[2] = {n_out, rows};
+    const cuuint64_t strides[1] = {n_out * 4};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t es[2] = {1, 1};
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, y, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return mfail(XMC_ERR_DEVICE, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return XMC_OK;
+}
+
 template <int BN, class Epi>
 int set_smem_attr() {
     static bool done = false;  // per template instance; set once per process (attribute is per function)
@@ -434,8 +452,44 @@ int wgrad_splits(const xmc_mlp* m, int l, int rows) {
     return std::min(s, kblocks);
 }
 
+bool fused_forward_ok(const xmc_mlp* m) {
+    return m->spec.forward_kernel == 0 && m->spec.n_out % 4 == 0 && m->L <= fused::kMaxL && m->in[0] == kInPad;
+}
+
+// Inference forward over `rows` rows of m->x into m->y with the fused kernel (mlp_fused.cuh).
+int enqueue_fused_forward(xmc_mlp* m, int rows) {
+    static bool attr = false;
+    if (!attr) {
+        XM_CUDA(cudaFuncSetAttribute(fused::mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     fused::kSmemBytes));
+        attr = true;
+    }
+    fused::Params p;
+    std::memset(&p, 0, sizeof(p));
+    int st = make_map(&p.x, m->x, (uint64_t)rows, (uint64_t)kInPad, tc::kBM);
+    for (int l = 0; !st && l < m->L; ++l) {
+        st = make_map(&p.w[l], m->w16[l], (uint64_t)m->out[l], (uint64_t)m->in[l], l < m->L - 1 ? m->spec.hidden : 256);
+        p.bias[l] = m->b32[l];
+    }
+    if (!st) st = make_out_map(&p.y, m->y, (uint64_t)rows, (uint64_t)m->spec.n_out);
+    if (st) return st;
+    p.L = m->L;
+    p.hidden = m->spec.hidden;
+    p.out_chunks = m->out[m->L - 1] / 256;
+    p.n_tiles = rows / tc::kBM;
+    p.n_out = m->spec.n_out;
+    p.err = m->d_err;
+    int sms = 0;
+    XM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->spec.device));
+    const int grid = std::min(p.n_tiles, sms);
+    fused::mlp_forward_kernel<<<grid, fused::kThreads, fused::kSmemBytes, m->stream>>>(p);
+    XM_CUDA(cudaGetLastError());
+    return XMC_OK;
+}
+
 // Forward pass over `rows` rows of m->x (bf16, padded). Training: also Z, A^T, dY, loss.
 int enqueue_forward(xmc_mlp* m, int rows, bool train) {
+    if (!train && fused_forward_ok(m)) return enqueue_fused_forward(m, rows);
     const cudaStream_t st = m->stream;
     for (int l = 0; l < m->L; ++l) {
         const bf16* a_in = l == 0 ? m->x : m->a[l - 1];

@@ -189,4 +189,5 @@ class BatchResult(C.Structure):
 
 class MlpSpec(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("n_in", C.c_int32), ("hidden", C.c_int32), ("n_hidden", C.c_int32),
-                ("n_out", C.c_int32), ("max_rows", C.c_int32), ("device", C.c_int32), ("reserved", C.c_int32 * 9)]
+                ("n_out", C.c_int32), ("max_rows", C.c_int32), ("device", C.c_int32), ("forward_kernel", C.c_int32),
+                ("reserved", C.c_int32 * 8)]

@@ -32,11 +32,12 @@ class MLP:
     """n_in -> hidden x n_hidden (SiLU) -> n_out network on one GPU."""
 
     def __init__(self, n_in: int, n_out: int, hidden: int = 256, n_hidden: int = 4, max_rows: int = 65536,
-                 device: int = 0):
+                 device: int = 0, fused_forward: bool = True):
         self._lib = load()
         s = S.MlpSpec()
         s.struct_size = C.sizeof(S.MlpSpec)
         s.n_in, s.hidden, s.n_hidden, s.n_out, s.max_rows, s.device = n_in, hidden, n_hidden, n_out, max_rows, device
+        s.forward_kernel = 0 if fused_forward else 1
         self._m = C.c_void_p()
         check(self._lib.xmc_mlp_create(C.byref(s), C.byref(self._m)))
         self.n_in, self.n_out, self.hidden, self.n_hidden, self.max_rows = n_in, n_out, hidden, n_hidden, max_rows

@@ -8,11 +8,11 @@
 //   hidden 1..L-2  A = H [128 x hidden]   (shared memory)  B = W_l [hidden x hidden]
 //   output L-1     A = H                                   B = W_out, 256 output columns per chunk
 //
-// Roles (320 threads): warp 8 lane 0 issues the TMA loads (the X tile and the weights, 64 K-columns
-// per stage through a 2-stage ring); warp 9 lane 0 issues tcgen05.mma (M = 128, N = hidden or 256,
-// K = 16) into one of two 256-column TMEM accumulators, alternating, and commits to mbarriers;
-// warps 0-7 drain an accumulator with tcgen05.ld (warp w: TMEM lanes 32 (w % 4).., column half
-// w / 4). A hidden layer's epilogue adds the bias, applies SiLU and writes the BF16 activations
+// Roles (576 threads): warp 16 lane 0 issues the TMA loads (the X tile and the weights, 64
+// K-columns per stage through a 2-stage ring); warp 17 lane 0 issues tcgen05.mma (M = 128, N =
+// hidden or 256, K = 16) into one of two 256-column TMEM accumulators, alternating, and commits to
+// mbarriers; warps 0-15 drain an accumulator with tcgen05.ld (warp w: TMEM lanes 32 (w % 4).., a
+// quarter of the columns chosen by w / 4). A hidden layer's epilogue adds the bias, applies SiLU and writes the BF16 activations
 // back into H in the 128-byte-swizzled K-major layout the next layer's MMAs read (then
 // fence.proxy.async and an mbarrier arrive); the output epilogue adds the bias and stores 32 x 32
 // FP32 boxes through a swizzled staging buffer with TMA (cp.async.bulk.tensor store), so the
@@ -28,15 +28,16 @@ namespace xmc {
 namespace fused {
 
 constexpr int kMaxL = 9;
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 16;  // warp w reads TMEM lanes 32 (w % 4).. and column group w / 4
+constexpr int kColGroups = kEpiWarps / 4;
 constexpr int kThreads = 32 * (kEpiWarps + 2);
-constexpr int kWStages = 2;
+constexpr int kWStages = 2;  // weight ring depth (stages of 64 K-columns)
 constexpr int kXBytes = 128 * 64 * 2;      // input tile, one 64-column k-block
 constexpr int kKBlockBytes = 128 * 128;    // one 64-column k-block of a 128-row operand
 constexpr int kHBytes = 4 * kKBlockBytes;  // activations, hidden <= 256
 constexpr int kWBytes = 256 * 64 * 2;      // weight stage: up to 256 rows x 64 columns
 constexpr int kOutBox = 32 * 32 * 4;       // one warp's 32 x 32 FP32 output box
-constexpr int kOutBufs = 2;
+constexpr int kOutBufs = 1;  // output staging box per epilogue warp
 constexpr int kOffX = 0;
 constexpr int kOffH = kOffX + kXBytes;
 constexpr int kOffW = kOffH + kHBytes;
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_kernel(const __grid_c
         tc::mbar_wait(drain, 0, p.err);
     } else if (warp < kEpiWarps) {
         // ---------------- epilogue ----------------
-        const int quarter = warp & 3, half = warp >> 2;
+        const int quarter = warp & 3, group = warp >> 2;
         const int trow = quarter * 32 + lane;  // tile row of this thread (TMEM lane)
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         unsigned char* h_gen = gbase + kOffH;
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_kernel(const __grid_c
         for (int t = blockIdx.x; ok && t < p.n_tiles; t += gridDim.x) {
             for (int l = 0; ok && l < p.L; ++l) {
                 const bool hidden_l = l < p.L - 1;
-                const int cw = layer_n(p, l) / 2;  // this warp's columns of the chunk
+                const int cw = layer_n(p, l) / kColGroups;  // this warp's columns of the chunk
                 const float* bias = p.bias[l];
                 for (int c = 0; ok && c < layer_chunks(p, l); ++c, ++j) {
                     const uint32_t b = j & 1;
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_kernel(const __grid_c
                     tc::tc_fence_after();
 #pragma unroll 1
                     for (int cc = 0; cc < cw; cc += 32) {
-                        const int col = half * cw + cc;  // column within the chunk
+                        const int col = group * cw + cc;  // column within the chunk
                         // an output box wholly past n_out is neither staged nor stored, so that every
                         // staged buffer has its store committed (the buffer alternation relies on it)
                         if (!hidden_l && c * 256 + col >= p.n_out) continue;
@@ -267,7 +268,7 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_kernel(const __grid_c
                                              t * 128 + quarter * 32);
                                 bulk_commit();
                             }
-                            obuf ^= 1;
+                            obuf = obuf + 1 == kOutBufs ? 0 : obuf + 1;
                         }
                     }
                     tc::tc_fence_before();

@@ -259,6 +259,10 @@ def test_create_rejects_invalid_input_before_touching_the_device(tmp_path):
     m.info.numberOfLayers = 9
     assert lib.xmc_create(C.byref(m.info), None, C.byref(ctx)) == S.XMC_ERR_RANGE
     m.info.numberOfLayers = 4
+    for bad in (-2, 65537):  # crossing-log entries per thread: -1 (no log), 0 (default) .. 65536
+        o = api.options(trajectories=True, trajectory_log=bad)
+        assert lib.xmc_create(C.byref(m.info), C.byref(o), C.byref(ctx)) == S.XMC_ERR_RANGE
+        assert "trajectory_log" in _lib.last_error()
     m.info.surface[0].triangles[0].y = 99
     assert lib.xmc_create(C.byref(m.info), None, C.byref(ctx)) == S.XMC_ERR_INVALID_INPUT
     assert "vertex index" in _lib.last_error()

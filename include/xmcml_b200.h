@@ -215,6 +215,10 @@ typedef enum xmc_status {
                                           are walked again in a replay pass)                        */
 #define XMC_LARGE_GRID      (1u << 4)  /* accept Area partitions above 256 per axis (the reference wraps
                                           voxel indices at 256; this library indexes them in full)    */
+#define XMC_GPU_BVH         (1u << 5)  /* without input->bvhTree, build the BVH topology on the GPU (linear
+                                          BVH over Morton-sorted triangle centroids) instead of the
+                                          host's binned SAH: far faster to build for large meshes, a
+                                          little slower to traverse; xmc_run_noalloc ignores it      */
 
 typedef struct xmc_options {
     uint32_t struct_size;          /* sizeof(xmc_options); 0 selects all defaults                */
@@ -397,9 +401,10 @@ int xmc_layout_offsets(int64_t* out, int max_count);
 /* Self test of the kernel's ray query compiled for the host: for each ray (ox,oy,oz,dx,dy,dz in
  * rays[6*i]) the nearest hit with tmin <= t <= tmax over the device image of `input` (distance,
  * surface id or -1, unit normal or NULL), through the xy cell grid where the kernel would use it
- * (use_grid != 0) or the BVH only. Used by the CPU test suite. */
+ * (bit 0 of `flags`) or the BVH only; bit 1 builds the image's BVH on GPU 0 (XMC_GPU_BVH) instead
+ * of the host. Used by the test suites. */
 int xmc_debug_nearest(const InputInfo* input, int n_rays, const float* rays, float tmin, float tmax,
-                      float* t_out, int* surf_out, float* normal_out, int use_grid);
+                      float* t_out, int* surf_out, float* normal_out, int flags);
 
 /* Run the photon kernel's device-side self test: `n` Philox blocks for the given key written to
  * out[4*n] (device path), for comparing with xmc_philox4x32_10. */

@@ -175,7 +175,7 @@ void pad_box(float lo[3], float hi[3]) {
 
 }  // namespace
 
-bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err) {
+bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err, int gpu_device) {
     Builder B;
     int ntri = 0;
     std::vector<int> surf_base(in->numberOfSurfaces + 1, 0);
@@ -251,7 +251,37 @@ bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err) {
             B.nodes.clear();
         }
     }
-    if (!use_ref) {
+    if (!use_ref && gpu_device >= 0 && ntri >= 2) {
+        // Linear BVH topology from the GPU; subtrees of <= 4 triangles (contiguous in the sorted
+        // order) become leaves, boxes come from the vertices as for every other tree.
+        std::vector<int2> child, range;
+        if (!gpu_lbvh_topology(B.cen, ntri, gpu_device, &B.order, &child, &range, err)) return false;
+        B.nodes.reserve(2 * (size_t)ntri);
+        // post-order over the internal nodes with an explicit stack: (node, children done)
+        std::vector<int> built(ntri - 1, -1);
+        std::vector<std::pair<int, bool>> st{{0, false}};
+        auto leaf_of = [&](int c) { return B.make_leaf(-1 - c, -c); };
+        while (!st.empty()) {
+            auto [x, done] = st.back();
+            st.pop_back();
+            const int2 rg = range[x];
+            if (rg.y - rg.x + 1 <= 4) {
+                built[x] = B.make_leaf(rg.x, rg.y + 1);
+                continue;
+            }
+            const int2 c = child[x];
+            if (!done) {
+                st.push_back({x, true});
+                if (c.y >= 0) st.push_back({c.y, false});
+                if (c.x >= 0) st.push_back({c.x, false});
+                continue;
+            }
+            const int l = c.x >= 0 ? built[c.x] : leaf_of(c.x);
+            const int r = c.y >= 0 ? built[c.y] : leaf_of(c.y);
+            built[x] = B.make_inner(l, r);
+        }
+        root = built[0];
+    } else if (!use_ref) {
         B.order.resize(ntri);
         for (int t = 0; t < ntri; ++t) B.order[t] = t;
         root = B.build_sah(0, ntri, 0);

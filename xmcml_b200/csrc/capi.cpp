@@ -159,7 +159,8 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     img->opt = opt;
 
     std::string err;
-    if (!build_geometry(in, &img->geom, &err)) return fail(XMC_ERR_INVALID_INPUT, err);
+    if (!build_geometry(in, &img->geom, &err, (opt.flags & XMC_GPU_BVH) ? opt.device : -1))
+        return fail(err.rfind("GPU BVH", 0) == 0 ? XMC_ERR_DEVICE : XMC_ERR_INVALID_INPUT, err);
     const GeomImage& geom = img->geom;
 
     KParams& kp = img->kp;

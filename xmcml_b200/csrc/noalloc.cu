@@ -8,6 +8,7 @@
 // records, layer-transition table, detector records and the xy cell grid, plus the photon-id
 // dispenser and the status word) is scratch, and it lives here in one file-scope __device__ array of fixed size,
 // which every GPU that loads the library holds until the process exits.
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -64,7 +65,11 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
         return XMC_ERR_INVALID_INPUT;
     }
     HostImage img;
-    int st = prepare_image(input, opt, &img);
+    xmc_options o;  // the BVH is built on the host here: a GPU build would allocate device memory
+    xmc_default_options(&o);
+    if (opt && opt->struct_size) std::memcpy(&o, opt, std::min((size_t)opt->struct_size, sizeof(o)));
+    o.flags &= ~XMC_GPU_BVH;
+    int st = prepare_image(input, &o, &img);
     if (st) return st;
     if (img.kp.use_bias) {
         set_error("xmc_run_noalloc: biasing needs weight tables this entry point does not stage");

@@ -638,10 +638,14 @@ cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n
 
 // Host run of the kernel's ray query on the geometry image of `in` (self-test of the traversal).
 extern "C" int xmc_debug_nearest(const InputInfo* in, int n_rays, const float* rays, float tmin, float tmax,
-                                 float* t_out, int* surf_out, float* normal_out, int use_grid) {
+                                 float* t_out, int* surf_out, float* normal_out, int flags) {
     xmc::GeomImage g;
     std::string err;
-    if (!xmc::build_geometry(in, &g, &err)) { xmc::set_error(err); return XMC_ERR_INVALID_INPUT; }
+    const bool use_grid = (flags & 1) != 0;
+    if (!xmc::build_geometry(in, &g, &err, (flags & 2) ? 0 : -1)) {
+        xmc::set_error(err);
+        return (flags & 2) ? XMC_ERR_DEVICE : XMC_ERR_INVALID_INPUT;
+    }
     xmc::GridImage grid;
     if (use_grid) xmc::build_xy_grid(g, &grid);
     for (int r = 0; r < n_rays; ++r) {

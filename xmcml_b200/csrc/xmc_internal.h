@@ -240,7 +240,10 @@ int prepare_image(const InputInfo* in, const xmc_options* opt, HostImage* img);
 void fill_ledger(const unsigned long long* raw, uint32_t w0_fx, uint64_t n, xmc_ledger* led);
 
 // bvh.cpp
-bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err);
+// gpu_device >= 0 and no usable prebuilt tree: the BVH topology is built on that GPU (bvh_gpu.cu)
+bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err, int gpu_device = -1);
+bool gpu_lbvh_topology(const std::vector<float>& cen, int n, int device, std::vector<int>* order,
+                       std::vector<int2>* child, std::vector<int2>* range, std::string* err);
 // bvh.cpp: merged z-intervals occupied by the triangles of `g` (at most kMaxZSlabs, conservative)
 int occupied_z_slabs(const GeomImage& g, float* lo, float* hi);
 

@@ -117,6 +117,7 @@ XMC_NO_AREA_KILL = 1 << 1
 XMC_SCATTERING_MAP = 1 << 2
 XMC_DETECTOR_TRAJ = 1 << 3
 XMC_LARGE_GRID = 1 << 4
+XMC_GPU_BVH = 1 << 5
 
 
 class XmcOptions(C.Structure):

@@ -252,35 +252,65 @@ bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err, int g
         }
     }
     if (!use_ref && gpu_device >= 0 && ntri >= 2) {
-        // Linear BVH topology from the GPU; subtrees of <= 4 triangles (contiguous in the sorted
-        // order) become leaves, boxes come from the vertices as for every other tree.
-        std::vector<int2> child, range;
-        if (!gpu_lbvh_topology(B.cen, ntri, gpu_device, &B.order, &child, &range, err)) return false;
-        B.nodes.reserve(2 * (size_t)ntri);
-        // post-order over the internal nodes with an explicit stack: (node, children done)
-        std::vector<int> built(ntri - 1, -1);
-        std::vector<std::pair<int, bool>> st{{0, false}};
-        auto leaf_of = [&](int c) { return B.make_leaf(-1 - c, -c); };
-        while (!st.empty()) {
-            auto [x, done] = st.back();
-            st.pop_back();
-            const int2 rg = range[x];
-            if (rg.y - rg.x + 1 <= 4) {
-                built[x] = B.make_leaf(rg.x, rg.y + 1);
-                continue;
-            }
-            const int2 c = child[x];
-            if (!done) {
-                st.push_back({x, true});
-                if (c.y >= 0) st.push_back({c.y, false});
-                if (c.x >= 0) st.push_back({c.x, false});
-                continue;
-            }
-            const int l = c.x >= 0 ? built[c.x] : leaf_of(c.x);
-            const int r = c.y >= 0 ? built[c.y] : leaf_of(c.y);
-            built[x] = B.make_inner(l, r);
+        // Linear BVH topology from the GPU over the ordinary triangles. Triangles far larger than the
+        // median (the planes of a layer stack) would sit in deep leaves with scene-sized boxes under a
+        // spatial-median split, so they get their own binned-SAH subtree beside it, at the root.
+        std::vector<float> ext(ntri);
+        for (int t = 0; t < ntri; ++t) {
+            float lo[3], hi[3];
+            B.tri_box(t, lo, hi);
+            ext[t] = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
         }
-        root = built[0];
+        std::vector<float> sorted_ext(ext);
+        std::nth_element(sorted_ext.begin(), sorted_ext.begin() + ntri / 2, sorted_ext.end());
+        const float big = 16.0f * sorted_ext[ntri / 2];
+        std::vector<int> small, large;
+        for (int t = 0; t < ntri; ++t) (big > 0.0f && ext[t] > big ? large : small).push_back(t);
+        const int ns = (int)small.size();
+        B.order.clear();
+        int root_s = -1;
+        if (ns >= 2) {
+            std::vector<float> cen_s(3 * (size_t)ns);
+            for (int i = 0; i < ns; ++i)
+                for (int k = 0; k < 3; ++k) cen_s[3 * (size_t)i + k] = B.cen[3 * (size_t)small[i] + k];
+            std::vector<int> order_s;
+            std::vector<int2> child, range;
+            if (!gpu_lbvh_topology(cen_s, ns, gpu_device, &order_s, &child, &range, err)) return false;
+            B.order.resize(ns);
+            for (int i = 0; i < ns; ++i) B.order[i] = small[order_s[i]];
+            B.nodes.reserve(2 * (size_t)ntri);
+            // post-order over the internal nodes with an explicit stack: (node, children done);
+            // subtrees of <= 4 triangles (contiguous in the sorted order) become leaves
+            std::vector<int> built(ns - 1, -1);
+            std::vector<std::pair<int, bool>> st{{0, false}};
+            auto leaf_of = [&](int c) { return B.make_leaf(-1 - c, -c); };
+            while (!st.empty()) {
+                auto [x, done] = st.back();
+                st.pop_back();
+                const int2 rg = range[x];
+                if (rg.y - rg.x + 1 <= 4) {
+                    built[x] = B.make_leaf(rg.x, rg.y + 1);
+                    continue;
+                }
+                const int2 c = child[x];
+                if (!done) {
+                    st.push_back({x, true});
+                    if (c.y >= 0) st.push_back({c.y, false});
+                    if (c.x >= 0) st.push_back({c.x, false});
+                    continue;
+                }
+                const int l = c.x >= 0 ? built[c.x] : leaf_of(c.x);
+                const int r = c.y >= 0 ? built[c.y] : leaf_of(c.y);
+                built[x] = B.make_inner(l, r);
+            }
+            root_s = built[0];
+        } else if (ns == 1) {
+            B.order.push_back(small[0]);
+            root_s = B.make_leaf(0, 1);
+        }
+        for (int t : large) B.order.push_back(t);
+        const int root_l = large.empty() ? -1 : B.build_sah(ns, ntri, 0);
+        root = root_s < 0 ? root_l : root_l < 0 ? root_s : B.make_inner(root_l, root_s);
     } else if (!use_ref) {
         B.order.resize(ntri);
         for (int t = 0; t < ntri; ++t) B.order[t] = t;

@@ -4,8 +4,8 @@
 // mcml_intersection.cpp:88-344), which for a 2 x 130,050-triangle height field takes a large part of
 // a second. Here the topology comes from the parallel construction of Karras (2012, "Maximizing
 // parallelism in the construction of BVHs, octrees, and k-d trees"):
-//   1. each triangle gets a 64-bit key: the 30-bit Morton code of its centroid (10 bits per axis
-//      over the centroid bounds) above its index, so keys are unique;
+//   1. each triangle gets a 64-bit key: the 30-bit Morton code of its centroid (10 bits per axis,
+//      one cubic grid over the centroid bounds) above its index, so keys are unique;
 //   2. the keys are sorted (CUB radix sort);
 //   3. internal node i of the n - 1 derives, from the longest common key prefixes around position
 //      i, the key range it covers and the split inside it, and so its two children (internal nodes
@@ -95,8 +95,11 @@ bool gpu_lbvh_topology(const std::vector<float>& cen, int n, int device, std::ve
             lo[k] = std::min(lo[k], cen[3 * (size_t)t + k]);
             hi[k] = std::max(hi[k], cen[3 * (size_t)t + k]);
         }
-    float inv[3];
-    for (int k = 0; k < 3; ++k) inv[k] = hi[k] > lo[k] ? 1.0f / (hi[k] - lo[k]) : 0.0f;
+    // one scale for the three axes (cubic Morton cells): a thin axis (the depth of a layer stack)
+    // is then split only where its cells are as small as the others, not at every third level
+    const float ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    const float s = ext > 0.0f ? 1.0f / ext : 0.0f;
+    const float inv[3] = {s, s, s};
 
     float* d_cen = nullptr;
     unsigned long long *d_keys = nullptr, *d_sorted = nullptr;

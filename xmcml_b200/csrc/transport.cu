@@ -178,14 +178,16 @@ __device__ __forceinline__ unsigned* xlog_row(const KParams& P, unsigned thread)
 __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, float x1, float y1, float z1,
                              unsigned long long w, int rdet, unsigned* __restrict__ xl, unsigned& xn) {
     if (z1 == z0) return;
+    // first plane at or above the lower end of the move; most moves cross none and stop here
+    const float step = P.plane_dz;
+    const int k = (int)fmaf(fminf(z0, z1) - P.az, P.asz, 0.5f);
+    float plane = P.az + k * step + 0.5f * step;
+    if (plane > fmaxf(z0, z1) || plane >= P.area_zend) return;
     float sx = x0, sy = y0, sz = z0, fz = z1, ex = x1 - x0, ey = y1 - y0, ez = z1 - z0;
     if (z1 < z0) {
         sx = x1; sy = y1; sz = z1; fz = z0;
         ex = -ex; ey = -ey; ez = -ez;
     }
-    const float step = P.plane_dz;
-    const int k = (int)((sz - P.az + 0.5f * step) / step);
-    float plane = P.az + k * step + 0.5f * step;
     const float inv = 1.0f / ez;
     for (int guard = 0; plane <= fz && plane < P.area_zend && guard < 65536; ++guard) {
         const float t = (plane - sz) * inv;

@@ -153,7 +153,6 @@ def cpu_reference_rate(xml, surf, seconds, threads, seed=777):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
     d = tempfile.mkdtemp(prefix="xmc_bench_ref_")
     inst = None
     if args.workload == "batch":

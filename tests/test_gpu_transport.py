@@ -99,7 +99,7 @@ def test_c1_reference_semantics(tmp_path):
 
 
 def test_c1_roulette_no_area_kill(tmp_path):
-    """BASELINE semantics: roulette 1e-4 / 0.1 and no Area kill; R + T + A + losses == 1 exactly."""
+    """Roulette semantics: roulette 1e-4 / 0.1 and no Area kill; R + T + A + losses == 1 exactly."""
     n = 100_000
     m, led, tal, out, oled, dw2, tw2 = _run_pair(tmp_path, scenes.planar(photons=n), n, roulette=True, area_kill=False)
     _check_exact(led, n)

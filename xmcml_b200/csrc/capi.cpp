@@ -1,6 +1,7 @@
 // C-ABI of the library: context creation (device image upload), runs, tally read-back and the
 // reference-signature shims. See include/xmcml_b200.h for the contract of each entry point.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -46,6 +47,8 @@ static void free_context(Context* c) {
     for (void* p : hbufs)
         if (p) cudaFreeHost(p);
     for (cudaEvent_t& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->map_ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->cancel_stream) cudaStreamDestroy(c->cancel_stream);
@@ -665,7 +668,9 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16;
     }
     // maps: one pinned staging buffer (kept by the context) for the scattering map and every
-    // detector's trajectory map, one copy each, then the additions into the caller's arrays
+    // detector's trajectory map. The trajectory maps are copied one by one, each followed by an
+    // event, and host threads (each owning a slice of the grid) add map d while later maps are still
+    // being copied; only the cells a photon crossed (non-zero counts) touch the caller's arrays.
     const bool want_scat = out && scat && out->scattering;
     const bool want_traj = out && traj;
     if (want_scat || want_traj) {
@@ -679,18 +684,46 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         }
         unsigned long long* hs = c->h_maps;
         unsigned long long* ht = c->h_maps + (want_scat ? (size_t)c->grid_size : 0);
+        const size_t G = (size_t)c->grid_size;
         if (want_scat) XMC_CUDA(cudaMemcpyAsync(hs, c->d_scatter, absorb_b, cudaMemcpyDeviceToHost, c->stream));
-        if (want_traj)
-            XMC_CUDA(cudaMemcpyAsync(ht, c->d_traj, absorb_b * (size_t)std::max(1, c->n_dets), cudaMemcpyDeviceToHost,
-                                     c->stream));
-        XMC_CUDA(cudaStreamSynchronize(c->stream));
-        if (want_scat) accumulate(out->scattering, hs, (size_t)c->grid_size, inv_scale);
-        if (want_traj)
-            for (int d = 0; d < c->n_dets; ++d) {
-                DetectorInfo& D = out->detectorInfo[d];
-                if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
-                accumulate(D.trajectory, ht + (size_t)d * c->grid_size, (size_t)c->grid_size, 0.0);
+        if (want_traj) {
+            while ((int)c->map_ev.size() < c->n_dets) {
+                cudaEvent_t e = nullptr;
+                XMC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                c->map_ev.push_back(e);
             }
+            const unsigned long long* dt = (const unsigned long long*)c->d_traj;
+            for (int d = 0; d < c->n_dets; ++d) {
+                XMC_CUDA(cudaMemcpyAsync(ht + d * G, dt + d * G, absorb_b, cudaMemcpyDeviceToHost, c->stream));
+                XMC_CUDA(cudaEventRecord(c->map_ev[d], c->stream));
+            }
+        }
+        if (want_scat) {
+            XMC_CUDA(want_traj && c->n_dets > 0 ? cudaEventSynchronize(c->map_ev[0]) : cudaStreamSynchronize(c->stream));
+            accumulate(out->scattering, hs, G, inv_scale);
+        }
+        if (want_traj && c->n_dets > 0) {
+            const unsigned hw = G < ((size_t)1 << 18) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+            std::atomic<int> failed{0};
+            auto worker = [&](unsigned t) {
+                if (cudaSetDevice(c->device) != cudaSuccess) { failed = 1; return; }
+                const size_t per = (G + hw - 1) / hw, a = std::min(G, t * per), b = std::min(G, a + per);
+                for (int d = 0; d < c->n_dets; ++d) {
+                    if (cudaEventSynchronize(c->map_ev[d]) != cudaSuccess) { failed = 1; return; }
+                    DetectorInfo& D = out->detectorInfo[d];
+                    if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
+                    const unsigned long long* src = ht + d * G;
+                    for (size_t i = a; i < b; ++i)
+                        if (src[i]) D.trajectory[i] += src[i];
+                }
+            };
+            std::vector<std::thread> pool;
+            for (unsigned t = 1; t < hw; ++t) pool.emplace_back(worker, t);
+            worker(0);
+            for (auto& th : pool) th.join();
+            if (failed) return fail(XMC_ERR_DEVICE, "trajectory map read-back failed");
+        }
+        XMC_CUDA(cudaStreamSynchronize(c->stream));
     }
     unsigned long long mismatch = 0;
     if (traj) {

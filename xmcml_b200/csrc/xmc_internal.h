@@ -168,6 +168,7 @@ struct Context {
     int block = 256, blocks_per_sm = 0, num_sms = 0, grid = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> map_ev;  // one per trajectory map: its read-back copy has landed
     // device buffers
     void* d_nodes = nullptr; void* d_tris = nullptr; void* d_next = nullptr; void* d_dets = nullptr;
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;

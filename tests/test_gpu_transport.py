@@ -483,3 +483,31 @@ def test_launch_keeps_context_only_for_unchanged_models(tmp_path):
     assert np.array_equal(b[0], fb[0]) and np.array_equal(b[1], fb[1])
     assert not np.array_equal(b[0], a1[0])
     _lib.check(_lib.load().xmc_launch_release())
+
+
+@pytest.mark.parametrize("partitions", [(100, 100, 100), (40, 40, 40)])
+def test_output_maps_accumulate_the_device_maps_exactly(tmp_path, partitions):
+    """xmc_run with an OutputInfo adds the run's maps into the caller's arrays (copied map by map and
+    added by host threads while later maps copy; 1e6 cells use several threads, 64,000 one): after
+    two runs every detector's trajectory map is exactly the sum of the two runs' integer maps, and the
+    scattering map their FP64 value."""
+    n = 30_000
+    sc = scenes.height_field_tissue(photons=n, grid=64, time_bins=10, area_partitions=partitions)
+    xml, surf = sc.write(str(tmp_path), "acc")
+    m = api.Model(xml, surf)
+    t = api.Transport(m, roulette=True, scattering=True, trajectories=True)
+    out = api.Output(m)
+    G, D = out.info.gridSize, m.n_detectors
+    traj_sum = np.zeros((D, G), dtype=np.uint64)
+    scat_sum = np.zeros(G, dtype=np.float64)
+    for seed in (3, 4):
+        t.run(n, seed=seed, output=out)
+        maps = t.maps()
+        traj_sum += maps["trajectory"][:D]
+        scat_sum += maps["scattering"].astype(np.float64) / WEIGHT_SCALE
+    t.close()
+    got = np.stack([np.ctypeslib.as_array(out.info.detectorInfo[d].trajectory, shape=(G,)) for d in range(D)])
+    assert traj_sum.sum() > 0
+    assert np.array_equal(got, traj_sum)
+    scat = np.ctypeslib.as_array(out.info.scattering, shape=(G,))
+    assert np.allclose(scat, scat_sum, rtol=1e-12, atol=0.0)

@@ -352,9 +352,11 @@ int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, uint64_t see
  * randomGenerator[0].value and the photons are ids 0..numberOfPhotons-1 (all of LaunchOMP's
  * tallies are filled, including the scattering map and the detector trajectory maps); afterwards
  * randomGenerator[0] is advanced by one MCG59 step, so consecutive calls (the reference's backup
- * portions, launcher_mpi.cpp:357-380) use fresh keys. numThreads is ignored. Default options
- * (reference semantics: weight cut at minWeight, photons killed outside Area). Returns 0 on
- * success; on failure it prints xmc_last_error() to stderr and returns the status. */
+ * portions, launcher_mpi.cpp:357-380) use fresh keys. numThreads is ignored. It runs on the
+ * calling thread's current CUDA device (cudaSetDevice), so one process per GPU, each with its own
+ * device selected, runs its own share. Default options otherwise (reference semantics: weight cut
+ * at minWeight, photons killed outside Area). Returns 0 on success; on failure it prints
+ * xmc_last_error() to stderr and returns the status. */
 int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* randomGenerator, int numThreads);
 
 /* Replaces InitOutput / FreeOutput (base/xmcml/xmcmlLauncher/launcher_omp.cpp:10-58, 76-104):

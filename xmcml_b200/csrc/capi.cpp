@@ -961,6 +961,8 @@ int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* rng, int numThre
     xmc_options opt;
     xmc_default_options(&opt);
     opt.flags = XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ;  // every tally LaunchOMP fills
+    int dev = 0;  // LaunchOMP has no device argument: the caller's current device
+    if (cudaGetDevice(&dev) == cudaSuccess) opt.device = dev;
     int st = xmc_launch(input, output, rng[0].value, 0, &opt, nullptr);
     if (st && st != XMC_ERR_BUDGET) {
         std::fprintf(stderr, "xmc_launch_omp: %s\n", xmc_last_error());

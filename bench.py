@@ -2,12 +2,15 @@
 
 Workload (default): the 3-layer tissue with the top two boundaries triangulated height fields
 (256 x 256 vertices over 20 x 20 mm each, 2 x 130,050 triangles, A = 0.05 mm, lam = 2 mm), planar
-L2/L3 boundary and bottom, 50 rings of 0.1 mm and 200 time bins of 5 ps, roulette 1e-4 / 0.1;
-one step = one transport call of 1e7 photons. Synthetic input generated by xmcml_b200.scenes.
+L2/L3 boundary and bottom, 50 rings of 0.1 mm and 200 time bins of 5 ps, 100^3 absorption grid;
+one step = one transport call of 1e7 photons with the reference LaunchOMP's semantics and tallies
+(weight cut at MinWeight 1e-4, photons killed outside Area, absorption grid, detectors, time bins,
+scattering map and one trajectory map per detector), so the GPU arms and the reference arm do the
+same work. Synthetic input generated by xmcml_b200.scenes.
 
   value : photons/s with the device image resident (xmc_run on a persistent context), device time
-          of every run from CUDA events on the library's stream (tally zeroing, kernel, read-back);
-          L2 is flushed between steps (256 MB write).
+          of every run from CUDA events on the library's stream (tally and map zeroing, run pass,
+          trajectory replay pass, tally read-back); L2 is flushed between steps (256 MB write).
   e2e   : photons/s through the reference-signature C-ABI xmc_launch_omp(InputInfo*, OutputInfo*,
           MCG59*, int) with host buffers (reference-layout BVH prebuilt once, as the reference's
           launcher does). Every step fingerprints the caller's InputInfo, runs, reads every tally
@@ -15,6 +18,8 @@ one step = one transport call of 1e7 photons. Synthetic input generated by xmcml
           tables, detectors) is built and uploaded only when the model's contents change, which
           `cold` measures (one call on a model the library has not seen). Host wall clock around
           the call.
+  workloads : the same measurements (fewer steps) on the planar 3-layer stack and on the ellipsoid
+          target scene, each with its own reference CPU baseline and roofline.
   --impl reference : the reference's own OpenMP LaunchOMP (compiled from its sources into
           oracle/_ref, -O3, all host threads) on a bounded sample of the same workload.
 Multi-GPU (torchrun): independent replicas on disjoint photon-id ranges (weak scaling); the only
@@ -40,6 +45,10 @@ METRIC = "photons/s (3-layer, BVH mesh)"
 UNIT = "photons/s"
 
 
+SEMANTICS = ("reference LaunchOMP: weight cut at MinWeight 1e-4, photons killed outside Area; absorption grid, "
+             "detectors, time bins, scattering map and one trajectory map per detector")
+
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -54,24 +63,30 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-surrogate", action="store_true")
+    p.add_argument("--extra-workloads", default="planar,ellipsoid",
+                   help="workloads measured beside the headline one (comma list, '' for none)")
+    p.add_argument("--extra-steps", type=int, default=3)
+    p.add_argument("--no-roulette-variant", action="store_true")
     return p.parse_args()
 
 
 def make_scene(workload, photons):
+    """Scene and config of a workload; the config is the same in every arm (ours and reference)."""
     from xmcml_b200 import scenes
     if workload == "heightfield":
         return scenes.height_field_tissue(photons=photons), {
             "workload": f"heightfield-3layer-256x256-{photons:.0e}", "surfaces": "2 height fields 256x256 (2x130050 tris) + 2 planes",
-            "rings": 50, "time_bins": "200 x 5 ps", "roulette": "1e-4 / 0.1", "grid": "100x100x100"}
+            "rings": 50, "time_bins": "200 x 5 ps", "grid": "100x100x100 over 10x10x5 mm",
+            "photons_per_step": photons, "semantics": SEMANTICS}
     if workload == "ellipsoid":
         sc = scenes.ellipsoid_target(photons=photons)
         return sc, {
             "workload": f"ellipsoid-target-3layer-{photons:.0e}", "surfaces": f"4 planes + icosphere ellipsoid 2x2x1 mm "
             f"({sc.n_triangles - 8} tris) at depth 2.5", "rings": 100, "time_bins": "200 x 5 ps",
-            "grid": "256x256x128 over 20x20x10 mm", "roulette": "1e-4 / 0.1"}
+            "grid": "256x256x128 over 20x20x10 mm", "photons_per_step": photons, "semantics": SEMANTICS}
     return scenes.planar(photons=photons), {
         "workload": f"planar-3layer-{photons:.0e}", "rings": 50, "grid": "100x100x100 over 10x10x5 mm",
-        "roulette": "1e-4 / 0.1"}
+        "photons_per_step": photons, "semantics": SEMANTICS}
 
 
 class ClockSampler:
@@ -161,8 +176,7 @@ def run_reference_arm(args, rank, world):
         from xmcml_b200 import batch as XB
         inst = XB.sample_instances(2024, args.instances, budget=(1e5 * args.budget_scale, 1e7 * args.budget_scale))
         sc = XB.to_scene(inst, 0)
-        cfg = {"workload": f"batched-{args.instances}-instances-3layer", "rings": 50, "time_bins": "20 x 50 ps",
-               "sample": "instance k at step k"}
+        cfg = batch_config(args, inst)
     else:
         sc, cfg = make_scene(args.workload, args.photons)
     xml, surf = sc.write(d, "bench")
@@ -192,20 +206,20 @@ def run_reference_arm(args, rank, world):
         OB.ref(True).ref_free_output(C.byref(out))
     tot = sum(times)
     value = n_step * args.steps / tot
-    cfg = dict(cfg)
-    cfg["parallelism"] = f"OpenMP x{threads} (host CPU)"
-    cfg["semantics"] = "reference: weight cut at MinWeight 1e-4, Area kill (no roulette in the reference)"
     metric = "photons/s (batched 3-layer instances)" if inst is not None else METRIC
     line = {"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "arm": {"parallelism": f"OpenMP x{threads} (host CPU)",
+                    "sample": ("instance k of the sweep at step k, " if inst is not None else "") +
+                              f"{n_step} photons per step"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{n_step} photons per step of the same workload, LaunchOMP with {threads} threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(args, m, N, rank, local, world, barrier, dist, torch):
+def run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch):
     """e2e photons/s through xmc_launch_omp with host InputInfo/OutputInfo (see module docstring).
 
     value: repeated LaunchOMP calls on one model (the library keeps the device image while the
@@ -226,7 +240,7 @@ def run_e2e(args, m, N, rank, local, world, barrier, dist, torch):
     cold_s = time.perf_counter() - t0
     barrier()
     e2e_t = []
-    for k in range(args.e2e_steps):
+    for k in range(e2e_steps):
         t0 = time.perf_counter()
         api.launch_omp(m, out, rng, 0)
         e2e_t.append(time.perf_counter() - t0)
@@ -235,7 +249,12 @@ def run_e2e(args, m, N, rank, local, world, barrier, dist, torch):
     dev = torch.device(f"cuda:{local}")
     e2e_s = replicas.max_over_ranks(sum(e2e_t), dist, dev)
     cold_s = replicas.max_over_ranks(cold_s, dist, dev)
-    e2e_value = world * args.e2e_steps * N / e2e_s
+    e2e_value = world * e2e_steps * N / e2e_s
+    lib.xmc_launch_release()
+    grid = out.info.gridSize
+    D = out.info.numberOfDetectors
+    T = m.info.timeScaleSize
+    out.close()
     # where a warm call's time goes: the same run through a context with LaunchOMP's options
     t = api.Transport(m, roulette=False, scattering=True, trajectories=True, device=local)
     out2 = api.Output(m)
@@ -246,12 +265,9 @@ def run_e2e(args, m, N, rank, local, world, barrier, dist, torch):
     image_b = led["h2d_bytes"]
     t.close()
     out2.close()
-    grid = out.info.gridSize
-    D = out.info.numberOfDetectors
-    T = m.info.timeScaleSize
     # read back per call: absorption, scattering and D trajectory maps (u64), detector and time-bin
-    # tallies (4 u64 each), two ledgers, status, replay count
-    d2h = 8 * grid * (2 + D) + 32 * D + 32 * D * T + 2 * 8 * 32 + 16 + 8
+    # tallies (4 u64 each), the run and replay ledgers, status
+    d2h = 8 * grid * (2 + D) + 32 * D + 32 * D * T + 2 * 8 * 32 + 16
     m.info.bvhTree = None
     lib.xmc_free_bvh_tree(tree)
     return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(d2h),
@@ -263,10 +279,26 @@ def run_e2e(args, m, N, rank, local, world, barrier, dist, torch):
             "breakdown_ms": {"kernels": led["kernel_ms"], "device_total": led["total_ms"], "host_wall": wall_ms,
                              "trajectory_replayed": led["n_trajectory_replayed"]}}
 
-def roofline(led, kernel_ms, clocks, n_photons):
-    """Issue-bound roofline of the transport kernel from the per-step cost model (48 FP32 flop,
-    6 MUFU and ~45 INT32 ops of Philox per walk iteration, plus 16 flop per BVH node test and
-    30 flop per triangle test), against the nominal SIMT peak 148 SMs x 128 lanes x SM clock."""
+
+def atomic_peak(local):
+    """Measured throughput of scattered 64-bit atomic adds into an L2-resident 8 MB array (the
+    tallies' access pattern) on this GPU, adds/s."""
+    from xmcml_b200 import _lib
+    rate, ms = C.c_double(0), C.c_double(0)
+    _lib.check(_lib.load().xmc_atomic_throughput(local, 20, 256, C.byref(rate), C.byref(ms)))
+    return rate.value
+
+
+def roofline(led, kernel_ms, clocks, n_photons, atomics_per_s=None, traj_adds=0):
+    """Roofline of the transport kernel from the per-step cost model, three roofs:
+      issue   : 48 FP32 flop + ~45 INT32 ops (Philox) per walk iteration, plus 16 flop per BVH/grid
+                node test and 30 per triangle test, against the nominal SIMT peak 148 SMs x 128
+                lanes x SM clock;
+      mufu    : 6 MUFU ops per iteration against 148 SMs x 16 MUFU lanes x SM clock;
+      atomics : one 64-bit absorption add per iteration (an upper bound: boundary iterations drop no
+                weight) plus one scattering-map add per z-plane crossing and one trajectory-map add
+                per crossing of a detected photon, against the measured L2 atomic throughput.
+    The largest fraction names the bound."""
     steps = led["steps"]
     nodes = led["n_node_visits"]
     tris = led["n_triangle_tests"]
@@ -277,17 +309,25 @@ def roofline(led, kernel_ms, clocks, n_photons):
     achieved = ops / t
     mufu = steps * 6 / t
     mufu_peak = 148 * 16 * sm_mhz * 1e6
-    # the step cost model's two compute roofs; the larger fraction names the bound (the walk's tally
-    # atomics have no measured peak here and are not claimed as a roof)
     roofs = {"issue": achieved / peak_ops, "mufu": mufu / mufu_peak}
+    adds = steps + led.get("n_plane_crossings", 0) + traj_adds
+    if atomics_per_s:
+        roofs["atomics"] = adds / t / atomics_per_s
     bound = max(roofs, key=roofs.get)
-    return {"bound": bound, "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TOP/s",
-            "frac": achieved / peak_ops, "traffic": None, "roofs": roofs,
+    if bound == "atomics":
+        head = {"achieved": adds / t / 1e9, "peak": atomics_per_s / 1e9, "unit": "G adds/s"}
+    elif bound == "mufu":
+        head = {"achieved": mufu / 1e12, "peak": mufu_peak / 1e12, "unit": "T MUFU ops/s"}
+    else:
+        head = {"achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TOP/s"}
+    return {"bound": bound, **head, "frac": roofs[bound], "traffic": None, "roofs": roofs,
             "model": {"ops_per_step": (48 + 45), "node_tests_per_step": nodes / max(steps, 1),
                       "triangle_tests_per_step": tris / max(steps, 1), "steps_per_photon": steps / max(n_photons, 1),
-                      "mufu_frac": mufu / mufu_peak,
-                      "peak_source": "nominal 148 SMs x 128 FP32/INT32 lanes x median sampled SM clock (MEASURED_PEAKS.json "
-                                     "has no SIMT figure; the walk is not HBM- or tensor-bound)"}}
+                      "atomic_adds_per_step": adds / max(steps, 1), "atomic_adds_per_s": adds / t,
+                      "atomic_peak_adds_per_s": atomics_per_s,
+                      "peak_source": "issue: nominal 148 SMs x 128 FP32/INT32 lanes x median sampled SM clock "
+                                     "(MEASURED_PEAKS.json has no SIMT figure; the walk is not HBM- or tensor-bound); "
+                                     "atomics: measured in this run (xmc_atomic_throughput, 8 MB array)"}}
 
 
 def surrogate_inference(local):
@@ -334,6 +374,15 @@ def surrogate_inference(local):
             "vs_mc_1e7_photon_evals": evals / mc_evals, "mc_evals_per_s_at_1e7_photons": mc_evals,
             "mc_batched_photons_per_s": mc_rate,
             "error_note": "accuracy of the trained ensemble is measured by xmcml_b200.surrogate_study, not here"}
+
+
+def batch_config(args, inst):
+    """Config of the batched sweep, the same in both arms."""
+    return {"workload": f"batched-{len(inst)}-instances-3layer", "photons_per_step": int(inst.photons.sum()),
+            "budgets": f"log-uniform [{1e5 * args.budget_scale:.0e}, {1e7 * args.budget_scale:.0e}]",
+            "rings": 50, "time_bins": "20 x 50 ps",
+            "semantics": "GPU: roulette 1e-4 / 0.1, no Area kill (the sweep's semantics); reference arm: its LaunchOMP "
+                         "(weight cut; the reference has no roulette) on instance k at step k"}
 
 
 def run_batch_workload(args, rank, world, local, dist, torch, barrier):
@@ -396,11 +445,9 @@ def run_batch_workload(args, rank, world, local, dist, torch, barrier):
     line = {"metric": "photons/s (batched 3-layer instances)", "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ker_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batched-{K}-instances-3layer", "photons_per_step": total,
-                       "budgets": f"log-uniform [{1e5 * args.budget_scale:.0e}, {1e7 * args.budget_scale:.0e}]",
-                       "rings": R, "time_bins": f"{T} x 50 ps", "roulette": "1e-4 / 0.1", "autotune": tune,
-                       "parallelism": f"replicas x{world} (disjoint instance sets)",
-                       "l2": "instance table re-uploaded and 24.6 MB of tallies zeroed every step"},
+            "config": batch_config(args, inst),
+            "arm": {"autotune": tune, "parallelism": f"replicas x{world} (disjoint instance sets)",
+                    "l2": "instance table re-uploaded and 24.6 MB of tallies zeroed every step"},
             "clocks": clocks,
             "e2e": {"value": world * args.steps * total / wall_s, "unit": UNIT,
                     "h2d_bytes_per_step": K * (32 + 5 * 48), "d2h_bytes_per_step": K * (R * T * 8 + R * 8 + 16 * 8) + 4,
@@ -440,52 +487,80 @@ def main():
             dist.destroy_process_group()
         return
 
-    from xmcml_b200 import api, _lib
-    from xmcml_b200 import structs as S
+    atom = None
+    try:
+        atom = atomic_peak(local)
+    except Exception:
+        atom = None
+    line = measure_transport(args, args.workload, args.photons, args.steps, args.warmup, args.e2e_steps, rank, world,
+                             local, dist, torch, barrier, atom, cpu_seconds=args.cpu_seconds)
+    if not args.no_roulette_variant:
+        # the same scene with roulette 1e-4 / 0.1 and no maps (the sweep's semantics), device time only
+        line["roulette_variant"] = measure_transport(args, args.workload, args.photons, args.extra_steps, 2, 0, rank,
+                                                     world, local, dist, torch, barrier, atom, roulette=True,
+                                                     cpu_seconds=0)
+    extra = {}
+    for wl in [w for w in args.extra_workloads.split(",") if w and w != args.workload]:
+        extra[wl] = measure_transport(args, wl, args.photons, args.extra_steps, 2, min(args.e2e_steps, 2), rank, world,
+                                      local, dist, torch, barrier, atom, cpu_seconds=args.cpu_seconds * 0.75)
+    if extra:
+        line["workloads"] = extra
+    if not args.no_surrogate:
+        try:
+            line["surrogate"] = surrogate_inference(local)
+        except Exception as e:  # reported, not fatal
+            line["surrogate"] = {"metric": "surrogate evals/s", "value": None, "error": str(e)}
+    line["gpu_launches"] = line["gpu_launches"] + sum(v["gpu_launches"] for v in extra.values()) + (
+        line["roulette_variant"]["gpu_launches"] if "roulette_variant" in line else 0)
+    line["gpu_launches_note"] = ("transport kernel launches (run pass + trajectory replay pass per call) of the timed "
+                                 "steps of the headline, the roulette variant and the extra workloads")
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, local, dist, torch, barrier, atom,
+                      roulette=False, cpu_seconds=12.0):
+    """Device-timed photons/s of `steps` transport calls of N photons on `workload` (L2 flushed
+    between steps), its roofline, the e2e rates through xmc_launch_omp and the reference's CPU rate
+    on the same scene. roulette=False: the reference LaunchOMP's semantics and tallies (the work the
+    reference arm does); True: roulette 1e-4 / 0.1 without maps."""
+    from xmcml_b200 import api, replicas
     d = tempfile.mkdtemp(prefix=f"xmc_bench_{rank}_")
-    sc, cfg = make_scene(args.workload, args.photons)
+    sc, cfg = make_scene(workload, N)
     xml, surf = sc.write(d, "bench")
     m = api.Model(xml, surf)
-    N = args.photons
-    t = api.Transport(m, roulette=True, device=local)
+    maps = not roulette
+    t = api.Transport(m, roulette=roulette, scattering=maps, trajectories=maps, device=local)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
-
-    from xmcml_b200 import replicas
-    for w in range(args.warmup):  # disjoint photon ids per rank and step
+    for w in range(warmup):  # disjoint photon ids per rank and step
         t.run(N, seed=777, first_photon=replicas.photon_range(rank, world, N, w)[0])
     barrier()
     leds = []
     with ClockSampler(local) as clk:
         barrier()
-        for k in range(args.steps):
+        for k in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
-            leds.append(t.run(N, seed=777, first_photon=replicas.photon_range(rank, world, N, args.warmup + k)[0]))
+            leds.append(t.run(N, seed=777, first_photon=replicas.photon_range(rank, world, N, warmup + k)[0]))
         barrier()
     clocks = clk.summary()
     dev = torch.device(f"cuda:{local}")
     dev_ms = replicas.max_over_ranks(sum(l["total_ms"] for l in leds), dist, dev)
     ker_ms = replicas.max_over_ranks(sum(l["kernel_ms"] for l in leds), dist, dev)
-    value = world * args.steps * N / (dev_ms / 1e3)
-    tal = t.tallies()
+    value = world * steps * N / (dev_ms / 1e3)
     last = leds[-1]
+    traj_adds = int(t.maps()["trajectory"].sum()) if maps else 0  # one atomic add per counted crossing
+    launches = sum(1 + (1 if l["n_trajectory_replayed"] > 0 else 0) for l in leds)
+    block = t.opts.block_size or 256
+    t.close()
+    del flush
 
-    # ---- e2e through the reference-signature C-ABI with host buffers ----
-    e2e = None
-    if args.e2e_steps > 0:
-        e2e = run_e2e(args, m, N, rank, local, world, barrier, dist, torch)
-    line_e2e = e2e
-
-    sur = None
-    if not args.no_surrogate:
-        try:
-            sur = surrogate_inference(local)
-        except Exception as e:  # reported, not fatal
-            sur = {"metric": "surrogate evals/s", "value": None, "error": str(e)}
-
-    rl = roofline(last, last["kernel_ms"], clocks, N)
-    prof = os.path.join(ROOT, "profiles", f"transport_kernel_{args.workload}_dram.json")
-    if os.path.exists(prof):
+    rl = roofline(last, last["kernel_ms"], clocks, N, atom, traj_adds)
+    prof = os.path.join(ROOT, "profiles", f"transport_kernel_{workload}_dram.json")
+    if os.path.exists(prof) and not roulette:
         try:
             pj = json.load(open(prof))
             rl["traffic"] = pj.get("dram_bytes_per_launch")
@@ -493,39 +568,42 @@ def main():
         except Exception:
             pass
 
+    e2e = None
+    if e2e_steps > 0:
+        e2e = run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch)
+
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_seconds > 0 and not args.no_cpu_baseline:
         try:
             from oracle import bind as OB
             if OB.ref_available(fast=True):
-                rate, n_cpu, secs = cpu_reference_rate(xml, surf, args.cpu_seconds, os.cpu_count() or 1)
+                rate, n_cpu, secs = cpu_reference_rate(xml, surf, cpu_seconds, os.cpu_count() or 1)
                 cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference",
                        "sample": f"{n_cpu} photons of the same workload through the reference's LaunchOMP "
-                                 f"({secs:.1f} s, -O3, reference semantics: weight cut, no roulette)"}
+                                 f"({secs:.1f} s, -O3, all tallies incl. scattering and trajectory maps)"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference", "sample": f"failed: {e}"}
-
-    cfg = dict(cfg)
-    cfg["photons_per_step"] = N
-    cfg["parallelism"] = f"replicas x{world} (disjoint photon ids)"
-    cfg["l2"] = "flushed between timed steps (256 MB write)"
-    cfg["launch"] = {"block": t.opts.block_size or 256}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic", "config": cfg, "clocks": clocks,
-            "e2e": line_e2e,
-            "gpu_launches": args.steps, "roofline": rl, "cpu_baseline": cpu, "surrogate": sur,
-            "kernel_ms_per_step": ker_ms / args.steps,
+    if cpu and cpu.get("value"):
+        cpu["gpu_value_over_cpu"] = value / cpu["value"]
+        if e2e:
+            cpu["gpu_e2e_over_cpu"] = e2e["value"] / cpu["value"]
+            cpu["gpu_e2e_cold_over_cpu"] = e2e["cold"]["value"] / cpu["value"]
+    m.close()
+    return {"metric": METRIC if workload == "heightfield" else f"photons/s ({workload})", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": cfg if not roulette else dict(cfg, semantics="roulette 1e-4 / 0.1, photons killed outside Area; "
+                                                                   "absorption grid, detectors and time bins (no maps)"),
+            "arm": {"parallelism": f"replicas x{world} (disjoint photon ids)", "launch": {"block": block},
+                    "l2": "flushed between timed steps (256 MB write)"},
+            "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": rl, "cpu_baseline": cpu,
+            "kernel_ms_per_step": ker_ms / steps,
             "walk": {"steps_per_photon": last["steps"] / N, "detected_fraction": last["n_detected"] / N,
                      "fp64_retests_per_step": last["n_fp64_retests"] / max(last["steps"], 1),
+                     "plane_crossings_per_step": last["n_plane_crossings"] / max(last["steps"], 1),
+                     "trajectory_replayed": last["n_trajectory_replayed"],
                      "escaped_top": last["escaped_top"], "absorbed": last["absorbed"],
                      "absorbed_target": last["absorbed_target"]}}
-    t.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

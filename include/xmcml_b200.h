@@ -269,6 +269,8 @@ typedef struct xmc_ledger {
     double bias_gained, bias_lost; /* the same per launched photon                               */
     uint64_t n_trajectory_replayed;/* XMC_DETECTOR_TRAJ: detected photons walked again because their
                                     * crossing log overflowed                                       */
+    uint64_t n_plane_crossings;    /* z-plane crossings through voxel centres recorded for the
+                                    * scattering / trajectory maps (run pass; 0 without maps)       */
 } xmc_ledger;
 
 typedef struct xmc_context xmc_context;
@@ -334,16 +336,25 @@ int xmc_launch(const InputInfo* input, OutputInfo* output, uint64_t seed,
  * The device copy of the model (BVH nodes, triangles, layer transitions, detectors, xy cell grid)
  * and the photon-id dispenser live in one static device array of XMC_NOALLOC_SCRATCH_BYTES (8 MiB)
  * that every GPU loading the library holds until exit; a model that needs more is rejected with
- * XMC_ERR_RANGE (a mesh of up to roughly 50,000 triangles fits). The first call on a device looks
- * up that array's device address, so make it once before any stream capture. All calls share the
- * array and it keeps the last call's contents: calls that overlap on the GPU (on different streams
- * or threads) race and must be serialised by the caller. `stream` is a cudaStream_t (NULL = the
- * default stream); the call returns after the run has finished on it. No host event, pinned buffer
- * or device allocation is made; the only host memory used is ordinary heap for the model image. */
+ * XMC_ERR_RANGE (a mesh of up to roughly 50,000 triangles fits). The first call on a device is its
+ * set-up: it looks up that array's device address (cudaGetSymbolAddress) and keeps it, so make that
+ * first call before any stream capture starts on the device. All calls share the array and it keeps
+ * the last call's contents: calls that overlap on the GPU (on different streams or threads) race and
+ * must be serialised by the caller. `stream` is a cudaStream_t (NULL = the default stream); each call
+ * copies the model into the array, runs, and waits for the run to finish on that stream before it
+ * returns. The caller's current device is unchanged on return. No host event, pinned buffer or
+ * device allocation is made; the only host memory used is ordinary heap for the model image. */
 #define XMC_NOALLOC_SCRATCH_BYTES (8u << 20)
 int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, uint64_t seed, uint64_t first_photon_id,
                     uint64_t n_photons, unsigned long long* d_absorption, unsigned long long* d_detectors,
                     unsigned long long* d_time_bins, unsigned long long* d_ledger, void* stream);
+
+/* No counterpart in the reference (a measurement utility): throughput of 64-bit atomic adds to
+ * scattered addresses of a device array of 2^log2_slots u64 (2^20 = 8 MB stays in L2), the access
+ * pattern of the walk's absorption-grid and map tallies; adds_per_thread per thread over a grid of
+ * 8 blocks of 256 threads per SM. Allocates and frees its own array on `device`. */
+int xmc_atomic_throughput(int device, unsigned log2_slots, unsigned adds_per_thread, double* atomics_per_s,
+                          double* ms);
 
 /* Replaces LaunchOMP(InputInfo*, OutputInfo*, MCG59*, int)
  * (base/xmcml/xmcmlLauncher/launcher_omp.h:10, launcher_omp.cpp:123-163): runs

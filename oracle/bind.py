@@ -46,8 +46,11 @@ class OracleLedger(C.Structure):
 
 
 def build(force: bool = False) -> None:
-    """Build liboracle.so (and _ref when the reference sources are present)."""
-    targets = ["oracle"] + (["ref"] if os.path.isdir("/root/reference") else [])
+    """Build liboracle.so, and _ref when the environment variable XMC_REFERENCE_DIR names a reference
+    checkout that is present."""
+    ref_dir = os.environ.get("XMC_REFERENCE_DIR", "")
+    with_ref = bool(ref_dir) and os.path.isdir(ref_dir)
+    targets = ["oracle"] + (["ref", f"REF={ref_dir}"] if with_ref else [])
     cmd = ["make", "-C", HERE] + (["-B"] if force else []) + targets
     subprocess.run(cmd, check=True, capture_output=True)
 

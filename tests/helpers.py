@@ -64,3 +64,46 @@ def oracle_opts_for(roulette=False, area_kill=True, beam_radius=0.0, nthreads=No
     flags = (B.OFLAG_ROULETTE if roulette else 0) | (0 if area_kill else B.OFLAG_NO_AREA_KILL)
     return B.default_opts(rng_kind=B.RNG_PHILOX, flags=flags, beam_radius=beam_radius,
                           nthreads=nthreads or os.cpu_count() or 1)
+
+
+class BatchStats:
+    """Running sum and sum of squares of a per-batch tally array over independent batches (photon-id
+    ranges or keys). The variance of the total is estimated from the spread of the batch values
+    (batch means): var(total) = B / (B - 1) * sum_b (x_b - total / B)^2."""
+
+    def __init__(self):
+        self.s1 = None
+        self.s2 = None
+        self.nz = None
+        self.k = 0
+
+    def add(self, x):
+        x = np.asarray(x, dtype=np.float64)
+        if self.s1 is None:
+            self.s1 = np.zeros_like(x)
+            self.s2 = np.zeros_like(x)
+            self.nz = np.zeros(x.shape, dtype=np.uint8)
+        self.s1 += x
+        self.s2 += x * x
+        self.nz += x != 0
+        self.k += 1
+
+    @property
+    def total(self):
+        return self.s1
+
+    def var_total(self):
+        k = self.k
+        if k < 2:
+            return np.full_like(self.s1, np.inf)
+        return np.maximum(self.s2 - self.s1 * self.s1 / k, 0.0) * k / (k - 1)
+
+
+def cell_zscores(g: BatchStats, o: BatchStats, min_batches=None):
+    """Per-cell z-scores of two batch-mean tallies over the cells that every batch of both sides
+    scored (so both variance estimates rest on all batches); returns (z of those cells, their count,
+    the number of cells either side scored)."""
+    kb = g.k if min_batches is None else min_batches
+    sel = (g.nz >= kb) & (o.nz >= kb)
+    z = zscores(g.total[sel], o.total[sel], g.var_total()[sel], o.var_total()[sel])
+    return z, int(sel.sum()), int(((g.nz > 0) | (o.nz > 0)).sum())

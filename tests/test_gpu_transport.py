@@ -511,3 +511,44 @@ def test_output_maps_accumulate_the_device_maps_exactly(tmp_path, partitions):
     assert np.array_equal(got, traj_sum)
     scat = np.ctypeslib.as_array(out.info.scattering, shape=(G,))
     assert np.allclose(scat, scat_sum, rtol=1e-12, atol=0.0)
+
+
+def test_entry_points_keep_the_callers_device_and_launch_omp_follows_it(tmp_path):
+    """Entry points that select a context's device restore the caller's current device on return, and
+    xmc_launch_omp runs on the calling thread's current device: on device 1 its tallies equal a device-0
+    run bit for bit, and switching back to device 0 rebuilds the kept context there. Needs 2 GPUs."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    n = 20_000
+    xml, surf = scenes.planar(photons=n).write(str(tmp_path), "dev")
+    m = api.Model(xml, surf)
+    lib = _lib.load()
+
+    def launch(dev):
+        torch.cuda.set_device(dev)
+        out = api.Output(m)
+        g = S.MCG59()
+        g.value, g.offset = 12345, 1
+        api.launch_omp(m, out, g, 0)
+        assert torch.cuda.current_device() == dev
+        return out.detector_weights(), out.absorption.copy()
+
+    _lib.check(lib.xmc_launch_release())
+    a0 = launch(0)
+    free1_before = torch.cuda.mem_get_info(1)[0]
+    a1 = launch(1)
+    assert torch.cuda.mem_get_info(1)[0] < free1_before  # the kept context now lives on device 1
+    assert np.array_equal(a0[0], a1[0]) and np.array_equal(a0[1], a1[1])
+    b0 = launch(0)
+    assert np.array_equal(a0[0], b0[0]) and np.array_equal(a0[1], b0[1])
+    # a context on device 1 used from device 0: every entry point leaves device 0 current
+    torch.cuda.set_device(0)
+    t = api.Transport(m, device=1)
+    assert torch.cuda.current_device() == 0
+    t.run(1000)
+    t.tallies()
+    assert torch.cuda.current_device() == 0
+    t.close()
+    assert torch.cuda.current_device() == 0
+    _lib.check(lib.xmc_launch_release())

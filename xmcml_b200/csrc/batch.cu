@@ -424,6 +424,7 @@ namespace xmc {
 namespace {
 
 void free_batch(xmc_batch* b) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!b) return;
     cudaSetDevice(b->spec.device);
     for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
@@ -629,6 +630,7 @@ extern "C" int xmc_batch_validate(const xmc_batch_spec* spec, const xmc_batch_in
 }
 
 extern "C" int xmc_batch_create(const xmc_batch_spec* spec, xmc_batch** out) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!out) return bfail(XMC_ERR_INVALID_INPUT, "out is NULL");
     *out = nullptr;
     if (!spec) return bfail(XMC_ERR_INVALID_INPUT, "spec is NULL");
@@ -684,6 +686,7 @@ extern "C" int xmc_batch_create(const xmc_batch_spec* spec, xmc_batch** out) {
 
 extern "C" int xmc_batch_run(xmc_batch* b, const xmc_batch_instance* inst, int n, double* ring_time, double* ring,
                              xmc_batch_result* result, double* kernel_ms) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!b) return bfail(XMC_ERR_INVALID_INPUT, "batch is NULL");
     int st = validate_instances(b->spec, inst, n);
     if (st) return st;
@@ -726,6 +729,7 @@ extern "C" int xmc_batch_run(xmc_batch* b, const xmc_batch_instance* inst, int n
 }
 
 extern "C" int xmc_batch_read_tallies(xmc_batch* b, int n, uint64_t* ring, uint64_t* ring_time, uint64_t* ledger) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!b) return bfail(XMC_ERR_INVALID_INPUT, "batch is NULL");
     if (n < 0 || n > b->last_n) return bfail(XMC_ERR_RANGE, "n exceeds the instance count of the last run");
     if (n == 0) return XMC_OK;
@@ -738,6 +742,7 @@ extern "C" int xmc_batch_read_tallies(xmc_batch* b, int n, uint64_t* ring, uint6
 }
 
 extern "C" int xmc_batch_set_tuning(xmc_batch* b, const xmc_batch_tuning* t) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!b || !t) return bfail(XMC_ERR_INVALID_INPUT, "batch or tuning is NULL");
     XB_CUDA(cudaSetDevice(b->spec.device));
     return apply_tuning(b, *t);
@@ -751,6 +756,7 @@ extern "C" int xmc_batch_get_tuning(const xmc_batch* b, xmc_batch_tuning* t) {
 
 extern "C" int xmc_batch_autotune(xmc_batch* b, const xmc_batch_instance* sample, int n, uint64_t photons_cap,
                                   xmc_batch_tuning* best) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!b) return bfail(XMC_ERR_INVALID_INPUT, "batch is NULL");
     int st = validate_instances(b->spec, sample, n);
     if (st) return st;

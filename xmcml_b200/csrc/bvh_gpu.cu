@@ -89,6 +89,7 @@ __global__ void karras_kernel(const unsigned long long* __restrict__ k, int n, i
 // range of sorted positions. Returns false with *err set on a CUDA failure.
 bool gpu_lbvh_topology(const std::vector<float>& cen, int n, int device, std::vector<int>* order,
                        std::vector<int2>* child, std::vector<int2>* range, std::string* err) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int t = 0; t < n; ++t)
         for (int k = 0; k < 3; ++k) {

@@ -1,7 +1,6 @@
 // C-ABI of the library: context creation (device image upload), runs, tally read-back and the
 // reference-signature shims. See include/xmcml_b200.h for the contract of each entry point.
 #include <algorithm>
-#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -34,6 +33,7 @@ static int fail(int status, const std::string& msg) {
     } while (0)
 
 static void free_context(Context* c) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!c) return;
     int dev = -1;
     if (cudaGetDevice(&dev) == cudaSuccess && dev != c->device) cudaSetDevice(c->device);
@@ -48,35 +48,40 @@ static void free_context(Context* c) {
         if (p) cudaFreeHost(p);
     for (cudaEvent_t& e : c->ev)
         if (e) cudaEventDestroy(e);
-    for (cudaEvent_t e : c->map_ev)
-        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->cancel_stream) cudaStreamDestroy(c->cancel_stream);
     delete c;
 }
 
-// dst[i] += src[i] * scale (scale != 0) or dst[i] += src[i] as integers, over n elements on up to 16
-// host threads (the caller's FP64 / u64 output arrays are large: up to detectors x voxels).
-template <typename D>
-static void accumulate(D* dst, const unsigned long long* src, size_t n, double scale) {
-    auto body = [&](size_t a, size_t b) {
-        for (size_t i = a; i < b; ++i) {
-            if constexpr (std::is_same<D, double>::value) dst[i] += (double)src[i] * scale;
-            else dst[i] += src[i];
-        }
-    };
-    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    if (n < (size_t)1 << 18 || hw == 1) {
-        body(0, n);
-        return;
-    }
+// Runs body(t) for t in [0, parts) on up to `parts` host threads, the calling thread included. When
+// the system cannot start a thread (std::system_error), the parts that got no thread run on the
+// calling thread, so no C++ exception crosses the C-ABI.
+template <typename F>
+static void parallel_parts(unsigned parts, F body) {
     std::vector<std::thread> pool;
-    const size_t per = (n + hw - 1) / hw;
-    for (unsigned t = 0; t < hw; ++t) {
-        const size_t a = t * per, b = std::min(n, a + per);
-        if (a < b) pool.emplace_back(body, a, b);
+    unsigned started = 1;
+    try {
+        for (; started < parts; ++started) pool.emplace_back(body, started);
+    } catch (...) {
     }
+    body(0);
+    for (unsigned t = started; t < parts; ++t) body(t);
     for (auto& th : pool) th.join();
+}
+
+static unsigned host_threads_for(size_t n) {
+    return n < ((size_t)1 << 18) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+}
+
+// dst[i] += src[i] * scale, over n elements on up to 16 host threads (the caller's FP64 output
+// arrays hold one value per voxel).
+static void accumulate(double* dst, const unsigned long long* src, size_t n, double scale) {
+    const unsigned hw = host_threads_for(n);
+    const size_t per = (n + hw - 1) / hw;
+    parallel_parts(hw, [&](unsigned t) {
+        const size_t a = std::min(n, t * per), b = std::min(n, a + per);
+        for (size_t i = a; i < b; ++i) dst[i] += (double)src[i] * scale;
+    });
 }
 
 // mcml_kernel.cpp:16-37 (FP64, exactly as the reference computes it)
@@ -383,6 +388,7 @@ void fill_ledger(const unsigned long long* L, uint32_t w0_fx, uint64_t n, xmc_le
     led->n_fp64_retests = L[L_N_RETEST];
     led->n_node_visits = L[L_N_NODES];
     led->n_triangle_tests = L[L_N_TRIS];
+    led->n_plane_crossings = L[L_N_CROSSINGS];
     led->specular_fx = (unsigned long long)(kWeightOne - w0_fx) * L[L_LAUNCHED];
     led->absorbed_fx = L[L_ABSORBED];
     led->absorbed_outside_fx = L[L_ABSORBED_OUT];
@@ -418,6 +424,7 @@ void fill_ledger(const unsigned long long* L, uint32_t w0_fx, uint64_t n, xmc_le
 }
 
 static int create(const InputInfo* in, const xmc_options* opt_in, Context** out) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     *out = nullptr;
     HostImage img;
     int st = prepare_image(in, opt_in, &img);
@@ -509,7 +516,7 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
     CK(cudaHostAlloc((void**)&c->h_absorb, absorb_b, cudaHostAllocDefault));
     CK(cudaHostAlloc((void**)&c->h_det, det_b, cudaHostAllocDefault));
     CK(cudaHostAlloc((void**)&c->h_tbin, tbin_b, cudaHostAllocDefault));
-    CK(cudaHostAlloc((void**)&c->h_ledger, led_b, cudaHostAllocDefault));
+    CK(cudaHostAlloc((void**)&c->h_ledger, 2 * led_b, cudaHostAllocDefault));  // run + replay ledgers
     CK(cudaHostAlloc((void**)&c->h_status, 16, cudaHostAllocDefault));
     kp.nodes = (const float4*)c->d_nodes;
     kp.tris = (const float4*)c->d_tris;
@@ -553,6 +560,7 @@ static int create(const InputInfo* in, const xmc_options* opt_in, Context** out)
 }
 
 static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo* out, xmc_ledger* led) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     XMC_CUDA(cudaSetDevice(c->device));
     KParams& kp = c->kp;
     kp.key0 = (uint32_t)seed;
@@ -563,6 +571,24 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, c->n_dets);
     const size_t tbin_b = det_b * c->n_time;
     const size_t led_b = sizeof(unsigned long long) * kLedgerSlots;
+    const bool traj = (c->opt.flags & XMC_DETECTOR_TRAJ) != 0;
+    const bool scat = (c->opt.flags & XMC_SCATTERING_MAP) != 0;
+    if (out) {
+        if (out->gridSize != c->grid_size) return fail(XMC_ERR_INVALID_INPUT, "output gridSize does not match the input Area");
+        if (out->numberOfDetectors != c->n_dets) return fail(XMC_ERR_INVALID_INPUT, "output numberOfDetectors does not match the input");
+    }
+    const bool want_scat = out && scat && out->scattering;
+    const bool want_traj = out && traj && c->n_dets > 0;
+    if (want_scat || want_traj) {  // pinned staging of the maps, kept by the context
+        const size_t need = absorb_b * ((want_scat ? 1 : 0) + (want_traj ? (size_t)c->n_dets : 0));
+        if (c->h_maps_bytes < need) {
+            if (c->h_maps) cudaFreeHost(c->h_maps);
+            c->h_maps = nullptr;
+            c->h_maps_bytes = 0;
+            XMC_CUDA(cudaHostAlloc((void**)&c->h_maps, need, cudaHostAllocDefault));
+            c->h_maps_bytes = need;
+        }
+    }
     XMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_absorb, 0, absorb_b, c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_det, 0, det_b, c->stream));
@@ -571,8 +597,6 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     XMC_CUDA(cudaMemsetAsync(c->d_counter, 0, 16, c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_status, 0, 16, c->stream));
     XMC_CUDA(cudaMemsetAsync(c->d_cancel, 0, 16, c->stream));
-    const bool traj = (c->opt.flags & XMC_DETECTOR_TRAJ) != 0;
-    const bool scat = (c->opt.flags & XMC_SCATTERING_MAP) != 0;
     if (scat) XMC_CUDA(cudaMemsetAsync(c->d_scatter, 0, absorb_b, c->stream));
     if (traj) {
         XMC_CUDA(cudaMemsetAsync(c->d_traj, 0, absorb_b * (size_t)std::max(1, c->n_dets), c->stream));
@@ -623,12 +647,24 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         kp.n_photons = n;
     }
     XMC_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    // Read-back: every copy is enqueued and waited for before anything is added into the caller's
+    // OutputInfo, so a failed copy returns with the output unchanged.
     if (out) XMC_CUDA(cudaMemcpyAsync(c->h_absorb, c->d_absorb, absorb_b, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaMemcpyAsync(c->h_det, c->d_det, det_b, cudaMemcpyDeviceToHost, c->stream));
     if (out) XMC_CUDA(cudaMemcpyAsync(c->h_tbin, c->d_tbin, tbin_b, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaMemcpyAsync(c->h_ledger, c->d_ledger, led_b, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaMemcpyAsync(c->h_status, c->d_status, 16, cudaMemcpyDeviceToHost, c->stream));
+    if (traj)
+        XMC_CUDA(cudaMemcpyAsync(c->h_ledger + kLedgerSlots, c->d_replay_ledger, led_b, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    // maps: one pinned staging buffer (allocated before the run) for the scattering map and every
+    // detector's trajectory map
+    unsigned long long* hs = c->h_maps;
+    unsigned long long* ht = c->h_maps + (want_scat ? (size_t)c->grid_size : 0);
+    const size_t G = (size_t)c->grid_size;
+    if (want_scat) XMC_CUDA(cudaMemcpyAsync(hs, c->d_scatter, absorb_b, cudaMemcpyDeviceToHost, c->stream));
+    if (want_traj)
+        XMC_CUDA(cudaMemcpyAsync(ht, c->d_traj, absorb_b * (size_t)c->n_dets, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaStreamSynchronize(c->stream));
     float k_ms = 0, t_ms = 0;
     XMC_CUDA(cudaEventElapsedTime(&k_ms, c->ev[1], c->ev[2]));
@@ -640,10 +676,7 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     const unsigned long long* L = c->h_ledger;
     const double inv_scale = 1.0 / kWeightScale;
     if (out) {
-        if (out->gridSize != c->grid_size) return fail(XMC_ERR_INVALID_INPUT, "output gridSize does not match the input Area");
-        if (out->numberOfDetectors != c->n_dets) return fail(XMC_ERR_INVALID_INPUT, "output numberOfDetectors does not match the input");
         out->specularReflectance = c->rsp;
-        if (out->absorption) accumulate(out->absorption, c->h_absorb, (size_t)c->grid_size, inv_scale);
         for (int d = 0; d < c->n_dets; ++d) {
             DetectorInfo& D = out->detectorInfo[d];
             const unsigned long long* t = c->h_det + 4 * (size_t)d;
@@ -659,6 +692,25 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
                 }
             }
         }
+        // voxel arrays on up to 16 host threads, each owning a slice of the grid: absorption and
+        // scattering (FP64 from fixed point) and every detector's trajectory map, where only the
+        // cells a photon crossed (non-zero counts) touch the caller's arrays
+        const unsigned hw = host_threads_for(G * (1 + (want_traj ? (size_t)c->n_dets : 0)));
+        const size_t per = (G + hw - 1) / hw;
+        parallel_parts(hw, [&](unsigned t) {
+            const size_t a = std::min(G, t * per), b = std::min(G, a + per);
+            if (out->absorption)
+                for (size_t i = a; i < b; ++i) out->absorption[i] += (double)c->h_absorb[i] * inv_scale;
+            if (want_scat)
+                for (size_t i = a; i < b; ++i) out->scattering[i] += (double)hs[i] * inv_scale;
+            for (int d = 0; want_traj && d < c->n_dets; ++d) {
+                DetectorInfo& D = out->detectorInfo[d];
+                if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
+                const unsigned long long* src = ht + d * G;
+                for (size_t i = a; i < b; ++i)
+                    if (src[i]) D.trajectory[i] += src[i];
+            }
+        });
     }
     if (led) {
         fill_ledger(L, c->w0_fx, n, led);
@@ -666,73 +718,7 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         led->total_ms = t_ms;
         led->h2d_bytes = c->h2d_bytes + sizeof(KParams);
         led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16;
-    }
-    // maps: one pinned staging buffer (kept by the context) for the scattering map and every
-    // detector's trajectory map. The trajectory maps are copied one by one, each followed by an
-    // event, and host threads (each owning a slice of the grid) add map d while later maps are still
-    // being copied; only the cells a photon crossed (non-zero counts) touch the caller's arrays.
-    const bool want_scat = out && scat && out->scattering;
-    const bool want_traj = out && traj;
-    if (want_scat || want_traj) {
-        const size_t need = absorb_b * ((want_scat ? 1 : 0) + (want_traj ? (size_t)std::max(1, c->n_dets) : 0));
-        if (c->h_maps_bytes < need) {
-            if (c->h_maps) cudaFreeHost(c->h_maps);
-            c->h_maps = nullptr;
-            c->h_maps_bytes = 0;
-            XMC_CUDA(cudaHostAlloc((void**)&c->h_maps, need, cudaHostAllocDefault));
-            c->h_maps_bytes = need;
-        }
-        unsigned long long* hs = c->h_maps;
-        unsigned long long* ht = c->h_maps + (want_scat ? (size_t)c->grid_size : 0);
-        const size_t G = (size_t)c->grid_size;
-        if (want_scat) XMC_CUDA(cudaMemcpyAsync(hs, c->d_scatter, absorb_b, cudaMemcpyDeviceToHost, c->stream));
-        if (want_traj) {
-            while ((int)c->map_ev.size() < c->n_dets) {
-                cudaEvent_t e = nullptr;
-                XMC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-                c->map_ev.push_back(e);
-            }
-            const unsigned long long* dt = (const unsigned long long*)c->d_traj;
-            for (int d = 0; d < c->n_dets; ++d) {
-                XMC_CUDA(cudaMemcpyAsync(ht + d * G, dt + d * G, absorb_b, cudaMemcpyDeviceToHost, c->stream));
-                XMC_CUDA(cudaEventRecord(c->map_ev[d], c->stream));
-            }
-        }
-        if (want_scat) {
-            XMC_CUDA(want_traj && c->n_dets > 0 ? cudaEventSynchronize(c->map_ev[0]) : cudaStreamSynchronize(c->stream));
-            accumulate(out->scattering, hs, G, inv_scale);
-        }
-        if (want_traj && c->n_dets > 0) {
-            const unsigned hw = G < ((size_t)1 << 18) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-            std::atomic<int> failed{0};
-            auto worker = [&](unsigned t) {
-                if (cudaSetDevice(c->device) != cudaSuccess) { failed = 1; return; }
-                const size_t per = (G + hw - 1) / hw, a = std::min(G, t * per), b = std::min(G, a + per);
-                for (int d = 0; d < c->n_dets; ++d) {
-                    if (cudaEventSynchronize(c->map_ev[d]) != cudaSuccess) { failed = 1; return; }
-                    DetectorInfo& D = out->detectorInfo[d];
-                    if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
-                    const unsigned long long* src = ht + d * G;
-                    for (size_t i = a; i < b; ++i)
-                        if (src[i]) D.trajectory[i] += src[i];
-                }
-            };
-            std::vector<std::thread> pool;
-            for (unsigned t = 1; t < hw; ++t) pool.emplace_back(worker, t);
-            worker(0);
-            for (auto& th : pool) th.join();
-            if (failed) return fail(XMC_ERR_DEVICE, "trajectory map read-back failed");
-        }
-        XMC_CUDA(cudaStreamSynchronize(c->stream));
-    }
-    unsigned long long mismatch = 0;
-    if (traj) {
-        unsigned long long rl[kLedgerSlots];
-        XMC_CUDA(cudaMemcpy(rl, c->d_replay_ledger, led_b, cudaMemcpyDeviceToHost));
-        mismatch = rl[L_N_REPLAY_MISMATCH];
-    }
-    if (led) {
-        led->n_replay_mismatch = mismatch;
+        led->n_replay_mismatch = traj ? c->h_ledger[kLedgerSlots + L_N_REPLAY_MISMATCH] : 0;
         led->n_trajectory_replayed = traj ? c->last_replayed : 0;
     }
     if (c->h_status[0] & 2) return fail(XMC_ERR_CANCELLED, "run cancelled");
@@ -777,6 +763,7 @@ int xmc_run(xmc_context* ctx, uint64_t seed, uint64_t first_photon_id, uint64_t 
 int xmc_read_tallies(xmc_context* ctx, uint64_t* absorption, uint64_t* det_weight, uint64_t* det_count,
                      uint64_t* det_target, uint64_t* det_weight2, uint64_t* time_weight, uint64_t* time_count,
                      uint64_t* time_target, uint64_t* time_weight2) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
     Context* c = reinterpret_cast<Context*>(ctx);
     XMC_CUDA(cudaSetDevice(c->device));
@@ -807,6 +794,7 @@ int xmc_read_tallies(xmc_context* ctx, uint64_t* absorption, uint64_t* det_weigh
 }
 
 int xmc_read_maps(xmc_context* ctx, uint64_t* scattering, uint64_t* trajectory) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!ctx) return fail(XMC_ERR_INVALID_INPUT, "context is NULL");
     Context* c = reinterpret_cast<Context*>(ctx);
     XMC_CUDA(cudaSetDevice(c->device));

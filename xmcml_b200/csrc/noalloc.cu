@@ -60,6 +60,7 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
                                uint64_t first_photon_id, uint64_t n_photons, unsigned long long* d_absorption,
                                unsigned long long* d_detectors, unsigned long long* d_time_bins,
                                unsigned long long* d_ledger, void* stream) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!d_absorption || !d_detectors || !d_time_bins || !d_ledger) {
         set_error("xmc_run_noalloc: output buffers must not be NULL");
         return XMC_ERR_INVALID_INPUT;

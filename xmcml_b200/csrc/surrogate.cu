@@ -424,6 +424,7 @@ namespace xmc {
 namespace {
 
 void free_mlp(xmc_mlp* m) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m) return;
     cudaSetDevice(m->spec.device);
     for (auto& kv : m->train_graphs) cudaGraphExecDestroy(kv.second);
@@ -594,6 +595,7 @@ int check_rows(const xmc_mlp* m, int rows) {
 }  // namespace xmc
 
 extern "C" int xmc_mlp_create(const xmc_mlp_spec* spec, xmc_mlp** out) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!spec || !out) return mfail(XMC_ERR_INVALID_INPUT, "spec or out is NULL");
     *out = nullptr;
     xmc_mlp_spec s{};
@@ -687,6 +689,7 @@ extern "C" int64_t xmc_mlp_param_count(const xmc_mlp* m) {
 // Flat parameter layout: for each layer W_l [out_l][in_l] row-major, then b_l [out_l], with
 // in_0 = n_in, out_{L-1} = n_out (no padding).
 extern "C" int xmc_mlp_set_params(xmc_mlp* m, const float* p) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m || !p) return mfail(XMC_ERR_INVALID_INPUT, "model or params is NULL");
     XM_CUDA(cudaSetDevice(m->spec.device));
     int in = m->spec.n_in;
@@ -733,6 +736,7 @@ static int copy_layers_out(const xmc_mlp* m, float* const* wsrc, float* const* b
 }
 
 extern "C" int xmc_mlp_get_params(const xmc_mlp* m, float* p) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m || !p) return mfail(XMC_ERR_INVALID_INPUT, "model or params is NULL");
     XM_CUDA(cudaSetDevice(m->spec.device));
     XM_CUDA(cudaStreamSynchronize(m->stream));
@@ -740,6 +744,7 @@ extern "C" int xmc_mlp_get_params(const xmc_mlp* m, float* p) {
 }
 
 extern "C" int xmc_mlp_forward(xmc_mlp* m, const float* x, int rows, float* y, double* ms) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m || !x || !y) return mfail(XMC_ERR_INVALID_INPUT, "model, x or y is NULL");
     int st = check_rows(m, rows);
     if (st) return st;
@@ -761,6 +766,7 @@ extern "C" int xmc_mlp_forward(xmc_mlp* m, const float* x, int rows, float* y, d
 // Times `reps` forward passes of the inputs already on the device (the last xmc_mlp_forward's),
 // replayed from a CUDA graph; *ms gets the mean device time of one pass.
 extern "C" int xmc_mlp_forward_timed(xmc_mlp* m, int rows, int reps, double* ms) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m || reps < 1) return mfail(XMC_ERR_INVALID_INPUT, "model is NULL or reps < 1");
     int st = check_rows(m, rows);
     if (st) return st;
@@ -798,6 +804,7 @@ extern "C" int xmc_mlp_forward_timed(xmc_mlp* m, int rows, int reps, double* ms)
 // Gradients of the mean squared error over `rows` rows at the current parameters (no update), in
 // the flat parameter layout; *loss gets the mean squared error.
 extern "C" int xmc_mlp_gradients(xmc_mlp* m, const float* x, const float* t, int rows, float* grads, float* loss) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m || !x || !t || !grads) return mfail(XMC_ERR_INVALID_INPUT, "NULL argument");
     int st = check_rows(m, rows);
     if (st) return st;
@@ -824,6 +831,7 @@ extern "C" int xmc_mlp_gradients(xmc_mlp* m, const float* x, const float* t, int
 }
 
 extern "C" int xmc_mlp_set_dataset(xmc_mlp* m, const float* x, const float* t, int rows) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m || !x || !t || rows < 1) return mfail(XMC_ERR_INVALID_INPUT, "NULL argument or empty data set");
     XM_CUDA(cudaSetDevice(m->spec.device));
     if (m->ds_x) cudaFree(m->ds_x);
@@ -852,6 +860,7 @@ extern "C" int xmc_mlp_set_dataset(xmc_mlp* m, const float* x, const float* t, i
 // Adam). losses[i] (may be NULL) gets the mean squared error of step i's minibatch.
 extern "C" int xmc_mlp_train(xmc_mlp* m, int steps, int batch, float lr, float beta1, float beta2, float eps,
                              uint64_t seed, float* losses, double* ms) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m || steps < 0) return mfail(XMC_ERR_INVALID_INPUT, "model is NULL or steps < 0");
     if (!m->ds_rows) return mfail(XMC_ERR_INVALID_INPUT, "no data set (xmc_mlp_set_dataset)");
     int st = check_rows(m, batch);
@@ -908,6 +917,7 @@ extern "C" int xmc_mlp_train(xmc_mlp* m, int steps, int batch, float lr, float b
 
 // Per-output weights of the squared error in training and in xmc_mlp_gradients (NULL: all 1).
 extern "C" int xmc_mlp_set_output_weights(xmc_mlp* m, const float* w) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (!m) return mfail(XMC_ERR_INVALID_INPUT, "model is NULL");
     XM_CUDA(cudaSetDevice(m->spec.device));
     XM_CUDA(cudaStreamSynchronize(m->stream));

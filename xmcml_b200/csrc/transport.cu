@@ -176,7 +176,8 @@ __device__ __forceinline__ unsigned* xlog_row(const KParams& P, unsigned thread)
 }
 
 __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, float x1, float y1, float z1,
-                             unsigned long long w, int rdet, unsigned* __restrict__ xl, unsigned& xn) {
+                             unsigned long long w, int rdet, unsigned* __restrict__ xl, unsigned& xn,
+                             unsigned& n_cross) {
     if (z1 == z0) return;
     // first plane at or above the lower end of the move; most moves cross none and stop here
     const float step = P.plane_dz;
@@ -193,6 +194,7 @@ __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, flo
         const float t = (plane - sz) * inv;
         const int idx = area_index(P, fmaf(ex, t, sx), fmaf(ey, t, sy), plane, 0.0f);
         if (idx < 0) break;
+        ++n_cross;
         if (P.mode == 0) {
             if (w && P.scatter) atomicAdd(&P.scatter[idx], (unsigned long long)w);
             if (xl) {
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     bool alive = false;
     Photon<WT> ph;
     ph.rdet = -1;
-    unsigned steps = 0, retests = 0, n_visit = 0, n_tri = 0;
+    unsigned steps = 0, retests = 0, n_visit = 0, n_tri = 0, n_cross = 0;
     unsigned long long bias_gained = 0, bias_lost = 0;
     unsigned long long absorbed = 0, absorbed_out = 0, absorbed_tgt = 0;  // per-thread sums, flushed at the end
     unsigned budget_hit = 0;
@@ -452,7 +454,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
         ph.py = fmaf(step, ph.dy, ph.py);
         ph.pz = fmaf(step, ph.dz, ph.pz);
         if (record_planes) cross_planes(P, ox, oy, oz, ph.px, ph.py, ph.pz, ph.w, ph.rdet,
-                                        log_traj ? xlog_row(P, threadIdx.x) : nullptr, xn);
+                                        log_traj ? xlog_row(P, threadIdx.x) : nullptr, xn, n_cross);
         ph.time = fmaf(step, L.n, ph.time);
         if (!(ph.pz > ph.gap_lo && ph.pz < ph.gap_hi)) find_gap(s_zlo, s_zhi, P.n_zocc, ph.pz, ph.gap_lo, ph.gap_hi);
         if ((P.target_mask >> ph.layer) & 1u) ph.trange += step;
@@ -576,6 +578,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     if (retests) atomicAdd(&S.ledger[L_N_RETEST], (unsigned long long)retests);
     atomicAdd(&S.ledger[L_N_NODES], (unsigned long long)n_visit);
     atomicAdd(&S.ledger[L_N_TRIS], (unsigned long long)n_tri);
+    if (n_cross) atomicAdd(&S.ledger[L_N_CROSSINGS], (unsigned long long)n_cross);
     if (budget_hit) atomicOr(P.status, 1);
     __syncthreads();
     for (int i = threadIdx.x; i < kLedgerSlots; i += blockDim.x) lat(&P.ledger[i], s_ledger[i]);
@@ -585,6 +588,53 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
 __global__ void philox_probe_kernel(uint32_t k0, uint32_t k1, unsigned long long pid, uint32_t n, uint4* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), i, 0u), k0, k1);
+}
+
+// Throughput of 64-bit atomic adds to scattered addresses of an L2-resident array (the tally
+// pattern of the walk: absorption voxels and map cells): each thread adds to `per_thread` slots
+// picked by a multiplicative hash of (thread, iteration).
+__global__ void atomic_probe_kernel(unsigned long long* slots, unsigned long long mask, unsigned per_thread) {
+    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long h = t * 0x9E3779B97F4A7C15ull;
+    for (unsigned i = 0; i < per_thread; ++i) {
+        h = (h ^ (h >> 29)) * 0xBF58476D1CE4E5B9ull + i;
+        atomicAdd(&slots[(h >> 17) & mask], 1ull);
+    }
+}
+
+cudaError_t atomic_throughput(int device, unsigned log2_slots, unsigned per_thread, double* atomics_per_s, double* ms_out) {
+    DeviceGuard guard;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    const size_t n = (size_t)1 << log2_slots;
+    unsigned long long* d = nullptr;
+    e = cudaMalloc(&d, n * sizeof(unsigned long long));
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a = nullptr, b = nullptr;
+    const dim3 grid(sms * 8), block(256);
+    float ms = 0.0f;
+    e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) e = cudaMemset(d, 0, n * sizeof(unsigned long long));
+    for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // the first launch warms up
+        cudaEventRecord(a);
+        atomic_probe_kernel<<<grid, block>>>(d, n - 1, per_thread);
+        cudaEventRecord(b);
+        e = cudaEventSynchronize(b);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    }
+    if (e == cudaSuccess) {
+        *atomics_per_s = (double)grid.x * block.x * per_thread / (ms * 1e-3);
+        *ms_out = ms;
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaFree(d);
+    return e;
 }
 
 cudaError_t enqueue_transport(Context* ctx) {
@@ -637,6 +687,21 @@ cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n
 }
 
 }  // namespace xmc
+
+// L2 atomic-add throughput of this GPU (roofline of the walk's tallies); allocates its own array.
+extern "C" int xmc_atomic_throughput(int device, unsigned log2_slots, unsigned adds_per_thread, double* atomics_per_s,
+                                     double* ms) {
+    if (!atomics_per_s || !ms || log2_slots < 10 || log2_slots > 30 || adds_per_thread == 0) {
+        xmc::set_error("xmc_atomic_throughput: bad arguments");
+        return XMC_ERR_INVALID_INPUT;
+    }
+    cudaError_t e = xmc::atomic_throughput(device, log2_slots, adds_per_thread, atomics_per_s, ms);
+    if (e != cudaSuccess) {
+        xmc::set_error(std::string("xmc_atomic_throughput: ") + cudaGetErrorString(e));
+        return XMC_ERR_DEVICE;
+    }
+    return XMC_OK;
+}
 
 // Host run of the kernel's ray query on the geometry image of `in` (self-test of the traversal).
 extern "C" int xmc_debug_nearest(const InputInfo* in, int n_rays, const float* rays, float tmin, float tmax,

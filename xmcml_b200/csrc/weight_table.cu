@@ -102,6 +102,7 @@ std::vector<double> distinct_anisotropies(const InputInfo* in) {
 
 int compute_weight_tables(const InputInfo* in, int device, std::vector<double>* gs, std::vector<double>* tables,
                           int* n_elem) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     if (in->weightTablePrecision < 1 || in->weightTablePrecision > (1u << 24))
         return wfail(XMC_ERR_RANGE, "weightTablePrecision must be in [1, 2^24]");
     if (in->weightIntegralPrecision < 1 || in->weightIntegralPrecision > 4096)

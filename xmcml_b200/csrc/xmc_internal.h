@@ -64,6 +64,7 @@ enum LedgerSlot {
     L_N_DETECTED, L_N_RETEST, L_N_NODES, L_N_TRIS,
     L_ABSORBED, L_ABSORBED_OUT, L_TOP, L_BOTTOM, L_AREA, L_CUT, L_GLASS, L_BUDGET, L_INVALID,
     L_RKILLED, L_RGAINED, L_N_REPLAY_MISMATCH, L_ABSORBED_TGT, L_BIAS_GAINED, L_BIAS_LOST,
+    L_N_CROSSINGS,
     L_COUNT
 };
 constexpr int kLedgerSlots = 32;  // padded
@@ -168,7 +169,6 @@ struct Context {
     int block = 256, blocks_per_sm = 0, num_sms = 0, grid = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    std::vector<cudaEvent_t> map_ev;  // one per trajectory map: its read-back copy has landed
     // device buffers
     void* d_nodes = nullptr; void* d_tris = nullptr; void* d_next = nullptr; void* d_dets = nullptr;
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
@@ -184,7 +184,8 @@ struct Context {
     int* h_cancel = nullptr;  // pinned source of the value xmc_cancel writes into d_cancel
     // pinned read-back buffers
     unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;
-    unsigned long long* h_tbin = nullptr; unsigned long long* h_ledger = nullptr;
+    unsigned long long* h_tbin = nullptr;
+    unsigned long long* h_ledger = nullptr;  // [2 x kLedgerSlots]: the run pass, then the replay pass
     unsigned long long* h_maps = nullptr;   // pinned staging of the scattering and trajectory maps (lazy)
     size_t h_maps_bytes = 0;
     int* h_status = nullptr;
@@ -259,5 +260,24 @@ cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm, bool
 cudaError_t device_philox(uint32_t key0, uint32_t key1, uint64_t pid, uint32_t n, uint32_t* host_out);
 
 void set_error(const std::string& msg);
+
+// Keeps the caller's current CUDA device across an entry point: the device current on entry is
+// made current again when the guard goes out of scope (every return path), so an entry point that
+// selects a context's device does not move the caller's later work (or xmc_launch_omp, which runs
+// on the current device) to another GPU.
+class DeviceGuard {
+  public:
+    DeviceGuard() { ok_ = cudaGetDevice(&prev_) == cudaSuccess; }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (ok_ && cudaGetDevice(&cur) == cudaSuccess && cur != prev_) cudaSetDevice(prev_);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+
+  private:
+    int prev_ = 0;
+    bool ok_ = false;
+};
 
 }  // namespace xmc

@@ -141,7 +141,8 @@ class XmcLedger(C.Structure):
                 + [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_uint64),
                    ("d2h_bytes", C.c_uint64), ("absorbed_target_fx", C.c_uint64), ("absorbed_target", C.c_double),
                    ("bias_gained_fx", C.c_uint64), ("bias_lost_fx", C.c_uint64), ("bias_gained", C.c_double),
-                   ("bias_lost", C.c_double), ("n_trajectory_replayed", C.c_uint64)])
+                   ("bias_lost", C.c_double), ("n_trajectory_replayed", C.c_uint64),
+                   ("n_plane_crossings", C.c_uint64)])
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

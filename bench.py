@@ -372,8 +372,35 @@ def surrogate_inference(local):
                          "issued_tflops": issued / (ms / 1e3) / 1e12,
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS 8192^3)"},
             "vs_mc_1e7_photon_evals": evals / mc_evals, "mc_evals_per_s_at_1e7_photons": mc_evals,
-            "mc_batched_photons_per_s": mc_rate,
-            "error_note": "accuracy of the trained ensemble is measured by xmcml_b200.surrogate_study, not here"}
+            "mc_batched_photons_per_s": mc_rate, "error": surrogate_accuracy(local)}
+
+
+def surrogate_accuracy(local, n_test=100, photons=1e7):
+    """Accuracy of the committed trained ensemble (xmcml_b200/data/surrogate_ensemble.npz, written by
+    xmcml_b200.surrogate_study --save) in this run: fresh held-out instances of the sweep's
+    distributions (a seed the training never used), their ring x time reflectance from the batched
+    Monte Carlo at `photons` each, and the network's median relative error on the cells the Monte
+    Carlo resolves to 1 %."""
+    import numpy as np
+    from xmcml_b200 import batch as XB
+    from xmcml_b200 import surrogate as SG
+    from xmcml_b200 import surrogate_study as SS
+    if not os.path.exists(SG.DEFAULT_ENSEMBLE):
+        return {"value": None, "note": f"{os.path.relpath(SG.DEFAULT_ENSEMBLE, ROOT)} missing"}
+    sur = SG.Surrogate.load(SG.DEFAULT_ENSEMBLE, device=local)
+    test = XB.sample_instances(90210, n_test, budget=(photons, photons), beam_radius=(0.0, 0.5))
+    b = XB.Batch(n_rings=50, ring_width=0.1, n_time=20, time_finish=1000 * XB.C_MM_PER_PS, max_instances=n_test,
+                 device=local)
+    rt, w2, ms = SS.run_batched(b, test, n_test)
+    b.close()
+    acc = SS.evaluate(sur, test, rt, w2, sur.floor)
+    sur.close()
+    return {"value": acc["median_rel_err_cells"], "unit": "median relative error (cells resolved to 1 %)",
+            "p90": acc["p90_rel_err_cells"], "rings": acc["median_rel_err_rings"],
+            "gate_pass_fraction": acc["gate_pass_fraction"], "gated": acc["median_rel_err_cells_gated"],
+            "judged_cells": acc["judged_cells"],
+            "reference": f"batched Monte Carlo, {n_test} held-out instances x {photons:.0e} photons ({ms / 1e3:.1f} s)",
+            "ensemble": os.path.relpath(SG.DEFAULT_ENSEMBLE, ROOT)}
 
 
 def batch_config(args, inst):

@@ -219,6 +219,9 @@ typedef enum xmc_status {
                                           BVH over Morton-sorted triangle centroids) instead of the
                                           host's binned SAH: far faster to build for large meshes, a
                                           little slower to traverse; xmc_run_noalloc ignores it      */
+#define XMC_LANE_QUERIES    (1u << 6)  /* short ray queries walk the xy cell grid lane by lane instead of
+                                          warp-cooperatively (same hits, same tallies bit for bit;
+                                          a launch-shape choice for the autotuner)                    */
 
 typedef struct xmc_options {
     uint32_t struct_size;          /* sizeof(xmc_options); 0 selects all defaults                */

@@ -77,7 +77,9 @@ def test_gradients_match_oracle(weighted):
             rel = np.linalg.norm(gg - rr) / np.linalg.norm(rr)
             cos = gg @ rr / (np.linalg.norm(gg) * np.linalg.norm(rr))
             print(f"layer {i} {name}: rel err {rel:.2e} cosine {cos:.6f}")
-            assert rel < 2e-2 and cos > 0.9998
+            # the oracle rounds to BF16 at the same points: what is left is FP32 accumulation order
+            # and the rare BF16 rounding flip it causes (measured <= 2e-3)
+            assert rel < 5e-3 and cos > 0.99999
     m.close()
 
 

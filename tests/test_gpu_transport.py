@@ -182,6 +182,35 @@ def test_bit_reproducible_across_launch_shapes(tmp_path):
             assert led[k + "_fx"] == res[0][1][k + "_fx"]
 
 
+@pytest.mark.parametrize("which", ["heightfield", "ellipsoid"])
+def test_cooperative_and_lane_queries_are_identical(tmp_path, which):
+    """The warp-cooperative grid query (default) and the lane-by-lane walk of the cells
+    (XMC_LANE_QUERIES) test the same candidates and keep the same nearest hit: every tally, both maps
+    and every ledger term are identical bit for bit, and so are the counts of cells visited and
+    triangles tested."""
+    n = 40_000
+    sc = (scenes.height_field_tissue(photons=n, grid=128, time_bins=20) if which == "heightfield"
+          else scenes.ellipsoid_target(photons=n, subdiv=4))
+    xml, surf = sc.write(str(tmp_path), "q" + which)
+    m = api.Model(xml, surf)
+    res = []
+    for lane in (False, True):
+        t = api.Transport(m, roulette=True, scattering=True, trajectories=which == "heightfield", lane_queries=lane)
+        led = t.run(n, seed=17)
+        res.append((t.tallies(), t.maps(), led))
+        t.close()
+    (ta, ma, la), (tb, mb, lb) = res
+    for k in ta:
+        assert np.array_equal(ta[k], tb[k]), k
+    for k in ma:
+        assert np.array_equal(ma[k], mb[k]), k
+    for k in S.LEDGER_TERMS:
+        assert la[k + "_fx"] == lb[k + "_fx"], k
+    for k in ("steps", "n_node_visits", "n_triangle_tests", "n_fp64_retests", "n_plane_crossings", "n_detected"):
+        assert la[k] == lb[k], k
+    assert la["n_triangle_tests"] > 0
+
+
 def test_split_runs_add_up(tmp_path):
     """Photons are identified by id: running [0, n) in two calls gives the same integer tallies."""
     n = 40_000

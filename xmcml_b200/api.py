@@ -102,12 +102,14 @@ class Output:
 def options(roulette: bool = False, area_kill: bool = True, beam_radius: float = 0.0, chance: float = 0.1,
             device: int = 0, block_size: int = 0, blocks_per_sm: int = 0, photons_per_chunk: int = 0,
             smem_nodes: int = 0, max_steps: int = 0, large_grid: bool = False, scattering: bool = False,
-            trajectories: bool = False, trajectory_log: int = 0, gpu_bvh: bool = False) -> S.XmcOptions:
+            trajectories: bool = False, trajectory_log: int = 0, gpu_bvh: bool = False,
+            lane_queries: bool = False) -> S.XmcOptions:
     o = S.XmcOptions()
     load().xmc_default_options(C.byref(o))
     o.flags = (S.XMC_ROULETTE if roulette else 0) | (0 if area_kill else S.XMC_NO_AREA_KILL) | \
               (S.XMC_LARGE_GRID if large_grid else 0) | (S.XMC_SCATTERING_MAP if scattering else 0) | \
-              (S.XMC_DETECTOR_TRAJ if trajectories else 0) | (S.XMC_GPU_BVH if gpu_bvh else 0)
+              (S.XMC_DETECTOR_TRAJ if trajectories else 0) | (S.XMC_GPU_BVH if gpu_bvh else 0) | \
+              (S.XMC_LANE_QUERIES if lane_queries else 0)
     o.roulette_chance = chance
     o.beam_radius = beam_radius
     o.device = device

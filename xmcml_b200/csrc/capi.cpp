@@ -98,13 +98,18 @@ static double specular(const LayerInfo* layer) {
     return r1;
 }
 
-static size_t smem_layout(int n_dets, int smem_nodes, int smem_tris, int smem_next) {
+// Dynamic shared memory of a transport block (the kernel's carve-up): block-private ledger and
+// detector tallies, staged BVH nodes and triangles, layers, detectors, the transition table and,
+// for warp-cooperative queries, one WarpQuery per warp.
+static size_t smem_layout(int n_dets, int smem_nodes, int smem_tris, int smem_next, int coop_warps) {
     size_t b = sizeof(unsigned long long) * (size_t)(kLedgerSlots + 4 * n_dets);
     b += sizeof(float4) * (size_t)(2 * smem_nodes + 3 * smem_tris);
     b += sizeof(DevLayer) * MAX_LAYERS;
     b += sizeof(DevDetector) * (size_t)n_dets;
     b += (size_t)smem_next;
-    return (b + 15) & ~(size_t)15;
+    b = (b + 15) & ~(size_t)15;
+    b += sizeof(WarpQuery) * (size_t)coop_warps;
+    return b;
 }
 
 static int validate(const InputInfo* in, const xmc_options& opt) {
@@ -297,7 +302,7 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     int smem_tris = geom.n_tris <= 256 ? geom.n_tris : 0;
     int smem_nodes = 0;
     if (opt.smem_nodes >= 0) {
-        size_t base = smem_layout(nd, 0, smem_tris, smem_next);
+        size_t base = smem_layout(nd, 0, smem_tris, smem_next, 0);
         if (base < smem_cap) smem_nodes = (int)std::min<size_t>((smem_cap - base) / 32, (size_t)geom.n_nodes);
         if (opt.smem_nodes > 0) smem_nodes = std::min(smem_nodes, opt.smem_nodes);
     }
@@ -315,7 +320,9 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.grid_nx = img->grid.nx;
     kp.grid_ny = img->grid.ny;
     kp.n_big = (int)(img->grid.big.size() / 4);
-    img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next);
+    kp.coop_query = (opt.flags & XMC_LANE_QUERIES) ? 0 : 1;
+    const int block = opt.block_size > 0 ? opt.block_size : 256;
+    img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next, kp.coop_query ? block / 32 : 0);
     // ---- biasing (mcml_kernel.cpp:325-440) ----
     kp.use_bias = in->useBiasing ? 1 : 0;
     for (int l = 0; l < MAX_LAYERS; ++l) kp.layer_wtab[l] = -1;

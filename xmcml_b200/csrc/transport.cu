@@ -208,6 +208,163 @@ __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, flo
     }
 }
 
+// Nearest hit with tmin <= t <= tmax of every querying lane's short segment, by the whole warp at once
+// (all 32 lanes call it; `need` marks the lanes with a query). The same candidates and the same
+// choice as grid_nearest (geom.cuh): the big triangles, then the triangles listed in the xy cells
+// under the segment, culled by the cells' and entries' z-ranges; the nearest distance wins and equal
+// distances keep the lower triangle index. Instead of each lane walking its own cells and entries
+// (serial loops whose trip counts differ from lane to lane), the warp flattens the work:
+//   1. each querying lane's cell rectangle (at most kGridMaxCells cells; more: `fallback`, the lane
+//      uses the BVH) and its big-triangle candidates;
+//   2. all (lane, cell) pairs of the warp, 32 per round: cell header and z-intervals loaded by one
+//      lane each, cells whose intervals miss the segment dropped, the rest compacted into a list;
+//   3. all (lane, entry) pairs of the kept cells, 32 per round: entry z-cull, the triangle test by
+//      one lane each, the packed (distance, triangle) minimum per querying lane in shared memory.
+// Each stage costs one dependent load round trip per 32 pairs instead of one per cell (or per four
+// entries) and lane, and every lane of the warp does useful tests.
+__device__ __forceinline__ unsigned long long pack_hit(float d, unsigned tri) {
+    return ((unsigned long long)__float_as_uint(d) << 32) | tri;
+}
+
+__device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, const float4* __restrict__ s_big,
+                                             const float4* __restrict__ s_tris, bool need, float ox, float oy, float oz,
+                                             float dx, float dy, float dz, float tmin, float tmax, int excl, Hit& hit,
+                                             bool& fallback, unsigned& retests, unsigned& n_visit, unsigned& n_tri) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    fallback = false;
+    int ncell = 0;
+    unsigned long long best = pack_hit(tmax, 0xffffffffu);
+    if (need) {
+        const float ex = fmaf(dx, tmax, ox), ey = fmaf(dy, tmax, oy), ez = fmaf(dz, tmax, oz);
+        const float fx0 = fminf(fmaxf((fminf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
+        const float fx1 = fminf(fmaxf((fmaxf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
+        const float fy0 = fminf(fmaxf((fminf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
+        const float fy1 = fminf(fmaxf((fmaxf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
+        const bool inside = fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)P.grid_nx && fy0 < (float)P.grid_ny;
+        const int i0 = max(0, (int)floorf(fx0)), i1 = min(P.grid_nx - 1, (int)floorf(fx1));
+        const int j0 = max(0, (int)floorf(fy0)), j1 = min(P.grid_ny - 1, (int)floorf(fy1));
+        const float zl = fminf(oz, ez), zh = fmaxf(oz, ez);
+        if (inside && (i1 - i0 + 1) * (j1 - j0 + 1) > kGridMaxCells) {
+            fallback = true;
+        } else {
+            for (int k = 0; k < P.n_big; ++k) {
+                const float4 en = s_big[4 * k];
+                if (en.y < zl || en.x > zh) continue;
+                const int t = f2i(en.z);
+                if (t == excl) continue;
+                ++n_tri;
+                const float d = tri_distance(s_big[4 * k + 1], s_big[4 * k + 2], s_big[4 * k + 3], ox, oy, oz, dx, dy, dz,
+                                             retests);
+                if (d >= tmin && d <= tmax) best = min(best, pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
+            }
+            if (inside) {
+                ncell = (i1 - i0 + 1) * (j1 - j0 + 1);
+                W.ij0[lane] = i0 | (j0 << 16);
+                W.w[lane] = i1 - i0 + 1;
+            }
+            W.o[lane] = make_float4(ox, oy, oz, tmin);
+            W.d[lane] = make_float4(dx, dy, dz, tmax);
+            W.z[lane] = make_float2(zl, zh);
+            W.excl[lane] = excl;
+        }
+    }
+    W.best[lane] = best;
+    // (lane, cell) pairs: exclusive scan of the cell counts
+    int incl = ncell;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int n_pairs = __shfl_sync(FULL, incl, 31);
+    W.coff[lane] = incl - ncell;
+    __syncwarp();
+    int nk = 0;
+    for (int base = 0; base < n_pairs; base += 32) {
+        const int k = base + lane;
+        bool keep = false;
+        uint2 cell = make_uint2(0u, 0u);
+        int own = 0;
+        if (k < n_pairs) {
+            // the pair's lane: the last lane whose offset is <= k (it has cells: the next offset is > k)
+            int lo = 0, hi = 31;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (W.coff[mid] <= k) lo = mid;
+                else hi = mid - 1;
+            }
+            own = lo;
+            const int loc = k - W.coff[own], ww = W.w[own], ij = W.ij0[own];
+            const unsigned ci = (unsigned)((ij >> 16) + loc / ww) * (unsigned)P.grid_nx + (unsigned)((ij & 0xffff) + loc % ww);
+            cell = __ldg(&P.cells[ci]);
+            const float4 za = __ldg(&P.cell_z[2 * ci]), zb = __ldg(&P.cell_z[2 * ci + 1]);
+            const float2 z = W.z[own];
+            ++n_visit;
+            keep = cell.y > 0 && !((za.y < z.x || za.x > z.y) && (za.w < z.x || za.z > z.y) &&
+                                   (zb.y < z.x || zb.x > z.y) && (zb.w < z.x || zb.z > z.y));
+        }
+        const unsigned km = __ballot_sync(FULL, keep);
+        if (keep) {
+            const int pos = nk + __popc(km & lt);
+            W.cell[pos] = cell;
+            W.owner[pos] = (unsigned char)own;
+        }
+        nk += __popc(km);
+    }
+    __syncwarp();
+    // (lane, entry) pairs over the kept cells: exclusive scan of their entry counts
+    int n_ent = 0;
+    for (int base = 0; base < nk; base += 32) {
+        const int c = base + lane;
+        const int cnt = c < nk ? (int)W.cell[c].y : 0;
+        int inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(FULL, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (c < nk) W.eoff[c] = n_ent + inc - cnt;
+        n_ent += __shfl_sync(FULL, inc, 31);
+    }
+    __syncwarp();
+    for (int base = 0; base < n_ent; base += 32) {
+        const int k = base + lane;
+        if (k < n_ent) {
+            int lo = 0, hi = nk - 1;  // the entry's cell: the last kept cell whose offset is <= k
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (W.eoff[mid] <= k) lo = mid;
+                else hi = mid - 1;
+            }
+            const int own = W.owner[lo];
+            const float4 en = __ldg(&P.cell_entries[W.cell[lo].x + (unsigned)(k - W.eoff[lo])]);
+            const float2 z = W.z[own];
+            const int t = f2i(en.z);
+            if (!(en.y < z.x || en.x > z.y) && t != W.excl[own]) {
+                float4 a, b, c;
+                if (t < P.smem_tris) {
+                    a = s_tris[3 * t]; b = s_tris[3 * t + 1]; c = s_tris[3 * t + 2];
+                } else {
+                    a = __ldg(&P.tris[3 * t]); b = __ldg(&P.tris[3 * t + 1]); c = __ldg(&P.tris[3 * t + 2]);
+                }
+                ++n_tri;
+                const float4 o = W.o[own], dd = W.d[own];
+                const float d = tri_distance(a, b, c, o.x, o.y, o.z, dd.x, dd.y, dd.z, retests);
+                if (d >= o.w && d <= dd.w) atomicMin(&W.best[own], pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
+            }
+        }
+    }
+    __syncwarp();
+    if (need && !fallback) {
+        const unsigned long long b = W.best[lane];
+        const unsigned t = (unsigned)(b & 0xffffffffu);
+        hit.tri = t == 0xffffffffu ? -1 : (int)t;
+        hit.t = t == 0xffffffffu ? tmax : __uint_as_float((unsigned)(b >> 32));
+    }
+    __syncwarp();  // W is reused by the next query round
+}
+
 template <class Ph>
 __device__ __forceinline__ void kill(const SmemTally& S, Ph& ph, bool& alive, int count_slot, int weight_slot) {
     atomicAdd(&S.ledger[count_slot], 1ull);
@@ -307,6 +464,8 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     DevLayer* s_layer = reinterpret_cast<DevLayer*>(s_tris + 3 * P.smem_tris);
     DevDetector* s_det = reinterpret_cast<DevDetector*>(s_layer + MAX_LAYERS);
     int8_t* s_next = reinterpret_cast<int8_t*>(s_det + P.n_dets);
+    const size_t fixed = (size_t)(reinterpret_cast<unsigned char*>(s_next + P.smem_next) - smem);
+    WarpQuery* s_wq = reinterpret_cast<WarpQuery*>(smem + ((fixed + 15) & ~(size_t)15)) + (threadIdx.x >> 5);
     __shared__ float s_zlo[kMaxZSlabs], s_zhi[kMaxZSlabs];
     __shared__ float4 s_big[4 * kMaxBigTriangles];
     for (int i = threadIdx.x; i < 4 * P.n_big; i += blockDim.x) s_big[i] = P.big[i];
@@ -405,45 +564,74 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             need = __ballot_sync(FULL, !alive && !exhausted);
         }
         if (__ballot_sync(FULL, alive) == 0u) break;
-        if (!alive) continue;
 
         // ---- one walk iteration (mcml_kernel.cpp:47-125) ----
-        if (ph.iter >= P.max_steps) {
-            budget_hit = 1;
-            kill(S, ph, alive, L_N_BUDGET, L_BUDGET);
-            continue;
-        }
-        const uint4 r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter, 0u), P.key0, P.key1);
-        ph.iter++;
-        steps++;
-        const DevLayer& L = s_layer[ph.layer];
-        float u_roulette;
-        bool boundary;
+        // Up to the ray query no lane leaves the iteration, so that every lane reaches the query
+        // converged (the warp-cooperative query needs all 32); lanes with no photon or a photon that
+        // ends before it only skip the work.
+        bool act = alive;
+        bool needq = false;
+        float u_roulette = 0.0f;
+        bool boundary = false;
         Hit hit;
-        float step;
-        if (L.glass) {
-            hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py, ph.pz,
-                              ph.dx, ph.dy, ph.dz, ph.tmin, INFINITY, ph.excl, retests, n_visit, n_tri);
-            boundary = true;
-            u_roulette = u24(r.y);
-            if (hit.tri < 0) {
-                kill(S, ph, alive, L_N_GLASS, L_GLASS);
-                continue;
+        hit.t = 0.0f;
+        hit.tri = -1;
+        float step = 0.0f;
+        uint4 r = make_uint4(0u, 0u, 0u, 0u);
+        const DevLayer* Lp = &s_layer[0];
+        if (act) {
+            if (ph.iter >= P.max_steps) {
+                budget_hit = 1;
+                kill(S, ph, alive, L_N_BUDGET, L_BUDGET);
+                act = false;
+            } else {
+                r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter, 0u), P.key0, P.key1);
+                ph.iter++;
+                steps++;
+                Lp = &s_layer[ph.layer];
+                if (Lp->glass) {
+                    hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
+                                      ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, INFINITY, ph.excl, retests, n_visit, n_tri);
+                    boundary = true;
+                    u_roulette = u24(r.y);
+                    if (hit.tri < 0) {
+                        kill(S, ph, alive, L_N_GLASS, L_GLASS);
+                        act = false;
+                    } else {
+                        step = hit.t;
+                    }
+                } else {
+                    step = -__logf(u24(r.x)) * Lp->inv_mut;  // mcml_kernel.cpp:618-631
+                    const float zend = fmaf(step + kStepExtend, ph.dz, ph.pz);
+                    if (fminf(ph.pz, zend) > ph.gap_lo && fmaxf(ph.pz, zend) < ph.gap_hi) {
+                        hit.tri = -1;  // the step stays inside a triangle-free z-gap: no surface to cross
+                        hit.t = step;
+                    } else {
+                        needq = true;
+                    }
+                }
             }
-            step = hit.t;
-        } else {
-            step = -__logf(u24(r.x)) * L.inv_mut;  // mcml_kernel.cpp:618-631
-            const float zend = fmaf(step + kStepExtend, ph.dz, ph.pz);
-            if (fminf(ph.pz, zend) > ph.gap_lo && fmaxf(ph.pz, zend) < ph.gap_hi) {
-                hit.tri = -1;  // the step stays inside a triangle-free z-gap: no surface to cross
-                hit.t = step;
-            } else if (!(P.grid_nx > 0 &&
-                         grid_nearest(P.cells, P.cell_z, P.cell_entries, s_big, P.n_big, P.grid_x0, P.grid_y0, P.grid_icx,
-                                      P.grid_icy, P.grid_nx, P.grid_ny, P.tris, s_tris, P.smem_tris, ph.px, ph.py, ph.pz, ph.dx,
-                                      ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri, hit))) {
+        }
+        if (P.grid_nx > 0 && P.coop_query) {
+            bool fb = false;
+            if (__any_sync(FULL, needq))
+                warp_grid_query(P, *s_wq, s_big, s_tris, needq, ph.px, ph.py, ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin,
+                                step + kStepExtend, ph.excl, hit, fb, retests, n_visit, n_tri);
+            if (needq && fb)
+                hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
+                                  ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
+        } else if (needq) {
+            if (!(P.grid_nx > 0 &&
+                  grid_nearest(P.cells, P.cell_z, P.cell_entries, s_big, P.n_big, P.grid_x0, P.grid_y0, P.grid_icx,
+                               P.grid_icy, P.grid_nx, P.grid_ny, P.tris, s_tris, P.smem_tris, ph.px, ph.py, ph.pz, ph.dx,
+                               ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri, hit))) {
                 hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
                                   ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
             }
+        }
+        if (!act) continue;
+        const DevLayer& L = *Lp;
+        if (!L.glass) {
             boundary = hit.tri >= 0;
             if (boundary) step = hit.t;
             u_roulette = boundary ? u24(r.z) : u24(r.w);

@@ -78,6 +78,25 @@ constexpr int kGridMaxCells = 4;
 constexpr int kBigTriangleCells = 64;
 constexpr int kMaxBigTriangles = 64;
 
+// Shared-memory scratch of one warp for the warp-cooperative grid query: the rays of the lanes that
+// query (origin + tmin, direction + tmax, segment z-range, excluded triangle, cell rectangle), the
+// per-lane cell offsets, the cells that survive the z-cull with their entry offsets, and one packed
+// (distance bits << 32 | triangle) minimum per lane.
+constexpr int kWarpQueryCells = 32 * kGridMaxCells;
+struct WarpQuery {
+    float4 o[32];
+    float4 d[32];
+    float2 z[32];
+    int excl[32];
+    int ij0[32];                      // i0 | j0 << 16
+    int w[32];                        // cells per row of the lane's rectangle
+    int coff[33];                     // exclusive scan of the lanes' cell counts
+    int eoff[kWarpQueryCells + 1];    // exclusive scan of the kept cells' entry counts
+    unsigned long long best[32];
+    uint2 cell[kWarpQueryCells];      // kept cells: first entry, entry count
+    unsigned char owner[kWarpQueryCells];
+};
+
 // z-intervals occupied by triangles (merged, padded, sorted): a step whose z-range lies strictly
 // inside a gap between them cannot cross any surface, so its ray query is skipped.
 constexpr int kMaxZSlabs = 24;
@@ -100,6 +119,8 @@ struct KParams {
     int n_big;
     float grid_x0, grid_y0, grid_icx, grid_icy;  // origin and 1 / cell size
     int grid_nx, grid_ny;
+    int coop_query;           // 1: grid queries run warp-cooperatively (WarpQuery scratch per warp in
+                              // shared memory); 0: each lane walks its own cells
     // layers
     DevLayer layer[MAX_LAYERS];
     int n_layers;

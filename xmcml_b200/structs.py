@@ -118,6 +118,7 @@ XMC_SCATTERING_MAP = 1 << 2
 XMC_DETECTOR_TRAJ = 1 << 3
 XMC_LARGE_GRID = 1 << 4
 XMC_GPU_BVH = 1 << 5
+XMC_LANE_QUERIES = 1 << 6
 
 
 class XmcOptions(C.Structure):

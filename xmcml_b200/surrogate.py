@@ -10,6 +10,7 @@ Monte Carlo as fallback. No counterpart in the reference.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Dict, List, Optional, Tuple
 
 import numpy as np
@@ -18,6 +19,11 @@ from . import structs as S
 from ._lib import check, load
 
 FP = C.POINTER(C.c_float)
+
+# The trained ensemble shipped with the package, written by `python -m xmcml_b200.surrogate_study
+# --save` (4 members trained on the batched Monte Carlo of the layered sweep, 1e6 photons per training
+# instance, 50 rings x 20 time bins of 50 ps).
+DEFAULT_ENSEMBLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "surrogate_ensemble.npz")
 
 
 def _f32(a) -> np.ndarray:
@@ -342,6 +348,50 @@ class Surrogate:
             j = int(np.argmin(mc_loss))
             out["features"], out["loss_mc"], out["mc_evals"] = fb[j], float(mc_loss[j]), len(fb)
         return out
+
+    # ---- persistence ----
+    def save(self, path: str) -> None:
+        """Write the ensemble to an .npz file: the standardisation, the training hull, the gate
+        settings, and per member the weights as BF16 bit patterns (the precision the tensor-core
+        kernels compute in) and the biases in FP32."""
+        dims = [self.n_in] + [self.hidden] * self.n_hidden + [self.n_out]
+        arrays = {"dims": np.array(dims, dtype=np.int64), "x_mean": self.x_mean, "x_std": self.x_std,
+                  "y_mean": self.y_mean, "y_std": self.y_std, "lo": self.lo, "hi": self.hi,
+                  "settings": np.array([self.floor, self.gate, self.hull_margin, self.gate_floor])}
+        for i, m in enumerate(self.members):
+            p = m.get_params()
+            w_parts, b_parts, o = [], [], 0
+            for l in range(len(dims) - 1):
+                nw = dims[l] * dims[l + 1]
+                w_parts.append(p[o:o + nw]); o += nw
+                b_parts.append(p[o:o + dims[l + 1]]); o += dims[l + 1]
+            arrays[f"w{i}"] = to_bf16_bits(np.concatenate(w_parts))
+            arrays[f"b{i}"] = np.concatenate(b_parts).astype(np.float32)
+        np.savez_compressed(path, **arrays)
+
+    @classmethod
+    def load(cls, path: str, max_rows: int = 65536, device: int = 0) -> "Surrogate":
+        """An ensemble written by `save`, ready for predict / reflectance / inverse_fit."""
+        z = np.load(path)
+        dims = [int(v) for v in z["dims"]]
+        members = sum(1 for k in z.files if k.startswith("w"))
+        floor, gate, hull_margin, gate_floor = (float(v) for v in z["settings"])
+        sur = cls(n_in=dims[0], n_out=dims[-1], members=members, hidden=dims[1], n_hidden=len(dims) - 2,
+                  max_rows=max_rows, device=device, floor=floor, gate=gate, hull_margin=hull_margin,
+                  gate_floor=gate_floor)
+        for k in ("x_mean", "x_std", "y_mean", "y_std", "lo", "hi"):
+            setattr(sur, k, np.asarray(z[k], dtype=np.float64))
+        for i, m in enumerate(sur.members):
+            w = from_bf16_bits(z[f"w{i}"])
+            b = np.asarray(z[f"b{i}"], dtype=np.float32)
+            parts, ow, ob = [], 0, 0
+            for l in range(len(dims) - 1):
+                nw = dims[l] * dims[l + 1]
+                parts += [w[ow:ow + nw], b[ob:ob + dims[l + 1]]]
+                ow += nw
+                ob += dims[l + 1]
+            m.set_params(np.concatenate(parts))
+        return sur
 
     def close(self):
         for m in self.members:

@@ -555,12 +555,15 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
     on the same scene. roulette=False: the reference LaunchOMP's semantics and tallies (the work the
     reference arm does); True: roulette 1e-4 / 0.1 without maps."""
     from xmcml_b200 import api, replicas
+    from xmcml_b200 import structs as S
     d = tempfile.mkdtemp(prefix=f"xmc_bench_{rank}_")
     sc, cfg = make_scene(workload, N)
     xml, surf = sc.write(d, "bench")
     m = api.Model(xml, surf)
     maps = not roulette
-    t = api.Transport(m, roulette=roulette, scattering=maps, trajectories=maps, device=local)
+    kw = dict(roulette=roulette, scattering=maps, trajectories=maps, device=local)
+    tuned, tune_ms = api.autotune(m, sample_photons=min(N, 1_000_000), **kw)  # the project's launch-shape autotuner
+    t = api.Transport(m, tuned)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
     for w in range(warmup):  # disjoint photon ids per rank and step
         t.run(N, seed=777, first_photon=replicas.photon_range(rank, world, N, w)[0])
@@ -581,7 +584,9 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
     last = leds[-1]
     traj_adds = int(t.maps()["trajectory"].sum()) if maps else 0  # one atomic add per counted crossing
     launches = sum(1 + (1 if l["n_trajectory_replayed"] > 0 else 0) for l in leds)
-    block = t.opts.block_size or 256
+    shape = {"block": tuned.block_size, "photons_per_claim": tuned.photons_per_chunk,
+             "queries": "lane by lane" if tuned.flags & S.XMC_LANE_QUERIES else "warp-cooperative",
+             "autotune_sample_ms": tune_ms}
     t.close()
     del flush
 
@@ -621,7 +626,7 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": cfg if not roulette else dict(cfg, semantics="roulette 1e-4 / 0.1, photons killed outside Area; "
                                                                    "absorption grid, detectors and time bins (no maps)"),
-            "arm": {"parallelism": f"replicas x{world} (disjoint photon ids)", "launch": {"block": block},
+            "arm": {"parallelism": f"replicas x{world} (disjoint photon ids)", "launch": shape,
                     "l2": "flushed between timed steps (256 MB write)"},
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": rl, "cpu_baseline": cpu,
             "kernel_ms_per_step": ker_ms / steps,

@@ -319,6 +319,16 @@ int xmc_cancel(xmc_context* ctx);
 
 int xmc_destroy(xmc_context* ctx);
 
+/* No counterpart in the reference (the project's autotuner of the transport kernel's launch shape).
+ * Builds the device image of `input` under `base` (its flags, device and semantics are kept) and
+ * times `sample_photons` photons (0 = 1e6) under every candidate shape: block size {128, 256, 512}
+ * at the occupancy maximum, photon ids a warp claims from the dispenser at a time {32, 64, 128},
+ * and the ray-query scheme (warp-cooperative, or lane by lane with XMC_LANE_QUERIES). *best gets
+ * `base` with the fastest shape, *best_ms (may be NULL) its kernel time. Every shape gives
+ * bit-identical tallies: a photon's random numbers and tally arithmetic do not depend on it. */
+int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sample_photons, xmc_options* best,
+                 double* best_ms);
+
 /* One call = create + run on a device context. The context of the last model is kept for the next
  * call when nothing its device image depends on has changed (a 64-bit fingerprint over the layers,
  * surfaces, detectors, Area, time bins, start, biasing fields, weight tables, caller BVH and options;

@@ -581,3 +581,25 @@ def test_entry_points_keep_the_callers_device_and_launch_omp_follows_it(tmp_path
     t.close()
     assert torch.cuda.current_device() == 0
     _lib.check(lib.xmc_launch_release())
+
+
+def test_autotune_picks_a_shape_with_identical_tallies(tmp_path):
+    """xmc_autotune times the candidate launch shapes (block size, photons per warp claim, query
+    scheme) on a sample and returns the fastest; a run with the tuned options gives the same tallies
+    as the default shape, bit for bit."""
+    n = 30_000
+    xml, surf = scenes.height_field_tissue(photons=n, grid=96, time_bins=20).write(str(tmp_path), "tune")
+    m = api.Model(xml, surf)
+    best, ms = api.autotune(m, sample_photons=20_000, roulette=True)
+    assert ms > 0 and best.block_size in (128, 256, 512) and best.photons_per_chunk in (32, 64, 128)
+    assert best.flags & S.XMC_ROULETTE
+    res = []
+    for opts in (api.options(roulette=True), best):
+        t = api.Transport(m, opts)
+        led = t.run(n, seed=3)
+        res.append((t.tallies(), led))
+        t.close()
+    for k in res[0][0]:
+        assert np.array_equal(res[0][0][k], res[1][0][k]), k
+    for k in S.LEDGER_TERMS:
+        assert res[0][1][k + "_fx"] == res[1][1][k + "_fx"]

@@ -56,6 +56,7 @@ def load(path: str | None = None) -> C.CDLL:
         "xmc_layout_offsets": (C.c_int, [P(C.c_int64), C.c_int]),
         "xmc_device_philox": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, P(C.c_uint32)]),
         "xmc_atomic_throughput": (C.c_int, [C.c_int, C.c_uint, C.c_uint, P(C.c_double), P(C.c_double)]),
+        "xmc_autotune": (C.c_int, [P(S.InputInfo), P(S.XmcOptions), C.c_uint64, P(S.XmcOptions), P(C.c_double)]),
         "xmc_generate_bvh_tree": (P(S.BVHTree), [P(S.Surface), C.c_int]),
         "xmc_free_bvh_tree": (None, [P(S.BVHTree)]),
         "xmc_debug_nearest": (C.c_int, [P(S.InputInfo), C.c_int, P(C.c_float), C.c_float, C.c_float,
@@ -118,5 +119,5 @@ EXPORTS = [
     "xmc_mlp_create", "xmc_mlp_param_count", "xmc_mlp_set_params", "xmc_mlp_get_params", "xmc_mlp_forward",
     "xmc_mlp_forward_timed", "xmc_mlp_gradients", "xmc_mlp_set_dataset", "xmc_mlp_train", "xmc_mlp_destroy",
     "xmc_mlp_set_output_weights", "xmc_weight_integral_table", "xmc_launch_release",
-    "xmc_gemm_bf16", "xmc_atomic_throughput",
+    "xmc_gemm_bf16", "xmc_atomic_throughput", "xmc_autotune",
 ]

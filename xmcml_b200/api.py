@@ -187,6 +187,17 @@ class Transport:
             pass
 
 
+def autotune(model: Model, sample_photons: int = 1_000_000, **kw) -> tuple:
+    """The transport kernel's fastest launch shape for `model` (xmc_autotune): options built from
+    `kw` (semantics, maps, device) with the tuned block size, photons per warp claim and query
+    scheme, and the sample's kernel ms."""
+    base = options(**kw)
+    best = S.XmcOptions()
+    ms = C.c_double(0.0)
+    check(load().xmc_autotune(C.byref(model.info), C.byref(base), sample_photons, C.byref(best), C.byref(ms)))
+    return best, ms.value
+
+
 def launch_omp(model: Model, output: Output, rng: S.MCG59, num_threads: int = 0) -> int:
     """LaunchOMP(InputInfo*, OutputInfo*, MCG59*, int) on the GPU (launcher_omp.cpp:123-163)."""
     st = load().xmc_launch_omp(C.byref(model.info), C.byref(output.info), C.byref(rng), num_threads)

@@ -430,20 +430,37 @@ void fill_ledger(const unsigned long long* L, uint32_t w0_fx, uint64_t n, xmc_le
     led->bias_lost = (double)led->bias_lost_fx * s;
 }
 
+// Host image of `in` with its weight tables (computed on the GPU when biasing needs them and the
+// caller gave none).
+static int full_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img) {
+    int st = prepare_image(in, opt_in, img);
+    if (st) return st;
+    if (img->need_wtab) {  // biasing without the caller's tables: compute them (weight_integral.cpp:34-65) on the GPU
+        std::vector<double> gs, tables;
+        int ne = 0;
+        st = compute_weight_tables(in, img->opt.device, &gs, &tables, &ne);
+        if (st) return st;
+        st = set_weight_tables(in, gs, tables, ne, img);
+        if (st) return st;
+    }
+    return XMC_OK;
+}
+
+static int create_from_image(const HostImage& img, Context** out);
+
 static int create(const InputInfo* in, const xmc_options* opt_in, Context** out) {
     xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
     *out = nullptr;
     HostImage img;
-    int st = prepare_image(in, opt_in, &img);
+    int st = full_image(in, opt_in, &img);
     if (st) return st;
-    if (img.need_wtab) {  // biasing without the caller's tables: compute them (weight_integral.cpp:34-65) on the GPU
-        std::vector<double> gs, tables;
-        int ne = 0;
-        st = compute_weight_tables(in, img.opt.device, &gs, &tables, &ne);
-        if (st) return st;
-        st = set_weight_tables(in, gs, tables, ne, &img);
-        if (st) return st;
-    }
+    return create_from_image(img, out);
+}
+
+// Device context (buffers, uploads, launch shape) from a host image.
+static int create_from_image(const HostImage& img, Context** out) {
+    xmc::DeviceGuard device_guard;  // the caller's current device is restored on return
+    *out = nullptr;
     const xmc_options& opt = img.opt;
     const GeomImage& geom = img.geom;
     const std::vector<int8_t>& next = img.next;
@@ -829,6 +846,57 @@ int xmc_cancel(xmc_context* ctx) {
 
 int xmc_destroy(xmc_context* ctx) {
     free_context(reinterpret_cast<Context*>(ctx));
+    return XMC_OK;
+}
+
+int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sample_photons, xmc_options* best,
+                 double* best_ms) {
+    if (!input || !best) return fail(XMC_ERR_INVALID_INPUT, "xmc_autotune: NULL argument");
+    set_error("");
+    DeviceGuard device_guard;
+    HostImage img;
+    int st = full_image(input, base, &img);
+    if (st) return st;
+    const uint64_t n = sample_photons ? sample_photons : 1000000ull;
+    const int blocks[] = {128, 256, 512};
+    const int chunks[] = {32, 64, 128};
+    double best_t = INFINITY;
+    xmc_options best_o = img.opt;
+    std::string last_err;
+    for (int coop = 1; coop >= 0; --coop) {
+        for (int b : blocks) {
+            for (int ch : chunks) {
+                // launch-shape fields only: the device image and the tally arithmetic stay the same
+                img.opt.block_size = b;
+                img.opt.blocks_per_sm = 0;
+                img.opt.photons_per_chunk = ch;
+                img.opt.flags = coop ? (img.opt.flags & ~XMC_LANE_QUERIES) : (img.opt.flags | XMC_LANE_QUERIES);
+                img.kp.flags = img.opt.flags;
+                img.kp.chunk = ch;
+                img.kp.coop_query = coop;
+                img.smem_bytes = smem_layout(img.n_dets, img.kp.smem_nodes, img.kp.smem_tris, img.kp.smem_next,
+                                             coop ? b / 32 : 0);
+                Context* c = nullptr;
+                st = create_from_image(img, &c);
+                if (st) {  // this shape cannot be resident (shared memory, registers): skip it
+                    last_err = g_last_error;
+                    continue;
+                }
+                xmc_ledger led;
+                st = run(c, 1, 0, std::max<uint64_t>(n / 4, 1), nullptr, &led);
+                if (!st || st == XMC_ERR_BUDGET) st = run(c, 2, 0, n, nullptr, &led);
+                free_context(c);
+                if (st && st != XMC_ERR_BUDGET) return st;
+                if (led.kernel_ms < best_t) {
+                    best_t = led.kernel_ms;
+                    best_o = img.opt;
+                }
+            }
+        }
+    }
+    if (!(best_t < INFINITY)) return fail(XMC_ERR_DEVICE, "xmc_autotune: no launch shape could run: " + last_err);
+    *best = best_o;
+    if (best_ms) *best_ms = best_t;
     return XMC_OK;
 }
 

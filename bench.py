@@ -67,6 +67,7 @@ def parse_args():
                    help="workloads measured beside the headline one (comma list, '' for none)")
     p.add_argument("--extra-steps", type=int, default=3)
     p.add_argument("--no-roulette-variant", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="default launch shape (profiling runs)")
     return p.parse_args()
 
 
@@ -562,7 +563,10 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
     m = api.Model(xml, surf)
     maps = not roulette
     kw = dict(roulette=roulette, scattering=maps, trajectories=maps, device=local)
-    tuned, tune_ms = api.autotune(m, sample_photons=min(N, 1_000_000), **kw)  # the project's launch-shape autotuner
+    if args.no_autotune:
+        tuned, tune_ms = api.options(**kw), None
+    else:  # the project's launch-shape autotuner
+        tuned, tune_ms = api.autotune(m, sample_photons=min(N, 1_000_000), **kw)
     t = api.Transport(m, tuned)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
     for w in range(warmup):  # disjoint photon ids per rank and step
@@ -584,7 +588,7 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
     last = leds[-1]
     traj_adds = int(t.maps()["trajectory"].sum()) if maps else 0  # one atomic add per counted crossing
     launches = sum(1 + (1 if l["n_trajectory_replayed"] > 0 else 0) for l in leds)
-    shape = {"block": tuned.block_size, "photons_per_claim": tuned.photons_per_chunk,
+    shape = {"block": tuned.block_size or 256, "photons_per_claim": tuned.photons_per_chunk,
              "queries": "lane by lane" if tuned.flags & S.XMC_LANE_QUERIES else "warp-cooperative",
              "autotune_sample_ms": tune_ms}
     t.close()

@@ -235,7 +235,7 @@ typedef struct xmc_options {
     int32_t  photons_per_chunk;    /* photon ids a warp claims at a time (0 = 64)                 */
     int32_t  smem_nodes;           /* BVH nodes staged in shared memory (-1 = none, 0 = auto)      */
     int32_t  trajectory_log;       /* XMC_DETECTOR_TRAJ: z-plane crossings logged per resident thread
-                                    * (0 = 1024, at most 65536; -1 = no log, every detected photon
+                                    * (0 = 4096, at most 65536; -1 = no log, every detected photon
                                     * is replayed)                                                 */
     int32_t  reserved[6];
 } xmc_options;

@@ -232,7 +232,7 @@ def test_split_runs_add_up(tmp_path):
 def test_scattering_and_trajectory_maps(tmp_path, which, log):
     """UpdatePhotonTrajectory / UpdateDetectorTrajectory (mcml_kernel.cpp:750-810): the scattering map
     (weight at every z-plane crossing through voxel centres) and, per detector, the crossing counts
-    of the photons it detected. GPU: each thread's crossing log (log = 0: 1024 entries), counted at
+    of the photons it detected. GPU: each thread's crossing log (log = 0: 4096 entries), counted at
     detection; a photon whose log overflows (log = 16: most of them) or every detected photon (log =
     -1: no log) is walked again by the replay pass."""
     n = 50_000

@@ -70,6 +70,7 @@ extern "C" int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, u
     xmc_default_options(&o);
     if (opt && opt->struct_size) std::memcpy(&o, opt, std::min((size_t)opt->struct_size, sizeof(o)));
     o.flags &= ~XMC_GPU_BVH;
+    o.flags |= XMC_LANE_QUERIES;  // the cooperative query's entry records would need more scratch
     int st = prepare_image(input, &o, &img);
     if (st) return st;
     if (img.kp.use_bias) {

@@ -218,10 +218,14 @@ __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, flo
 //      uses the BVH) and its big-triangle candidates;
 //   2. all (lane, cell) pairs of the warp, 32 per round: cell header and z-intervals loaded by one
 //      lane each, cells whose intervals miss the segment dropped, the rest compacted into a list;
-//   3. all (lane, entry) pairs of the kept cells, 32 per round: entry z-cull, the triangle test by
-//      one lane each, the packed (distance, triangle) minimum per querying lane in shared memory.
+//   3. all (lane, entry) pairs of the kept cells, 64 per round (two per lane): each entry record
+//      carries its triangle, so one load round trip gives the z-cull and the triangle test; the
+//      packed (distance, triangle) minimum per querying lane is kept in shared memory.
 // Each stage costs one dependent load round trip per 32 pairs instead of one per cell (or per four
 // entries) and lane, and every lane of the warp does useful tests.
+#ifndef XMC_FAT_UNROLL
+#define XMC_FAT_UNROLL 1
+#endif
 __device__ __forceinline__ unsigned long long pack_hit(float d, unsigned tri) {
     return ((unsigned long long)__float_as_uint(d) << 32) | tri;
 }
@@ -328,31 +332,40 @@ __device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, 
         n_ent += __shfl_sync(FULL, inc, 31);
     }
     __syncwarp();
-    for (int base = 0; base < n_ent; base += 32) {
-        const int k = base + lane;
-        if (k < n_ent) {
-            int lo = 0, hi = nk - 1;  // the entry's cell: the last kept cell whose offset is <= k
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (W.eoff[mid] <= k) lo = mid;
-                else hi = mid - 1;
-            }
-            const int own = W.owner[lo];
-            const float4 en = __ldg(&P.cell_entries[W.cell[lo].x + (unsigned)(k - W.eoff[lo])]);
-            const float2 z = W.z[own];
-            const int t = f2i(en.z);
-            if (!(en.y < z.x || en.x > z.y) && t != W.excl[own]) {
-                float4 a, b, c;
-                if (t < P.smem_tris) {
-                    a = s_tris[3 * t]; b = s_tris[3 * t + 1]; c = s_tris[3 * t + 2];
-                } else {
-                    a = __ldg(&P.tris[3 * t]); b = __ldg(&P.tris[3 * t + 1]); c = __ldg(&P.tris[3 * t + 2]);
+    // two pairs per lane in flight: each brings its entry and triangle (one 64-byte record) in one
+    // round trip
+    constexpr int kU = XMC_FAT_UNROLL;
+    for (int base = 0; base < n_ent; base += 32 * kU) {
+        float4 rec[kU][4];
+        int own[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int k = base + 32 * u + lane;
+            own[u] = -1;
+            if (k < n_ent) {
+                int lo = 0, hi = nk - 1;  // the entry's cell: the last kept cell whose offset is <= k
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (W.eoff[mid] <= k) lo = mid;
+                    else hi = mid - 1;
                 }
-                ++n_tri;
-                const float4 o = W.o[own], dd = W.d[own];
-                const float d = tri_distance(a, b, c, o.x, o.y, o.z, dd.x, dd.y, dd.z, retests);
-                if (d >= o.w && d <= dd.w) atomicMin(&W.best[own], pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
+                own[u] = W.owner[lo];
+                const float4* f = P.cell_fat + 4 * (size_t)(W.cell[lo].x + (unsigned)(k - W.eoff[lo]));
+#pragma unroll
+                for (int q = 0; q < 4; ++q) rec[u][q] = __ldg(f + q);
             }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (own[u] < 0) continue;
+            const float2 z = W.z[own[u]];
+            const float4 en = rec[u][0];
+            const int t = f2i(en.z);
+            if (en.y < z.x || en.x > z.y || t == W.excl[own[u]]) continue;
+            ++n_tri;
+            const float4 o = W.o[own[u]], dd = W.d[own[u]];
+            const float d = tri_distance(rec[u][1], rec[u][2], rec[u][3], o.x, o.y, o.z, dd.x, dd.y, dd.z, retests);
+            if (d >= o.w && d <= dd.w) atomicMin(&W.best[own[u]], pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
         }
     }
     __syncwarp();
@@ -823,6 +836,24 @@ cudaError_t atomic_throughput(int device, unsigned log2_slots, unsigned per_thre
     if (b) cudaEventDestroy(b);
     cudaFree(d);
     return e;
+}
+
+__global__ void gather_fat_kernel(const float4* __restrict__ entries, const float4* __restrict__ tris, size_t n,
+                                  float4* __restrict__ fat) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const float4 en = entries[e];
+    const size_t t = (size_t)(unsigned)__float_as_int(en.z);
+    fat[4 * e] = en;
+    fat[4 * e + 1] = tris[3 * t];
+    fat[4 * e + 2] = tris[3 * t + 1];
+    fat[4 * e + 3] = tris[3 * t + 2];
+}
+
+cudaError_t gather_fat_entries(const float4* entries, const float4* tris, size_t n_entries, float4* fat, cudaStream_t st) {
+    if (n_entries == 0) return cudaSuccess;
+    gather_fat_kernel<<<(unsigned)((n_entries + 255) / 256), 256, 0, st>>>(entries, tris, n_entries, fat);
+    return cudaGetLastError();
 }
 
 cudaError_t enqueue_transport(Context* ctx) {

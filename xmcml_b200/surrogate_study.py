@@ -74,7 +74,7 @@ def main(argv=None):
     p.add_argument("--test", type=int, default=200)
     p.add_argument("--test-photons", type=float, default=1e7)
     p.add_argument("--members", type=int, default=4)
-    p.add_argument("--steps", type=int, default=30000, help="Adam steps (sizes above 6 epochs of it get up to 2x)")
+    p.add_argument("--steps", type=int, default=30000, help="Adam steps per member")
     p.add_argument("--batch", type=int, default=4096)
     p.add_argument("--lr", type=float, default=2e-3)
     p.add_argument("--floor", type=float, default=1e-7)
@@ -82,7 +82,8 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=2024)
     p.add_argument("--device", type=int, default=0)
     p.add_argument("--unweighted", action="store_true", help="plain (unweighted) mean squared error")
-    p.add_argument("--save", default="", help="write the ensemble of --save-size (default the largest) to this .npz")
+    p.add_argument("--save", default="", help="write the ensemble of --save-size (default the largest) to this .npz "
+                                              "(the package ships xmcml_b200/data/surrogate_ensemble.npz)")
     p.add_argument("--save-size", type=int, default=0)
     p.add_argument("--out", default="")
     a = p.parse_args(argv)
@@ -106,7 +107,7 @@ def main(argv=None):
     curve, res = [], None
     save_size = a.save_size or n_train
     for size in sizes:
-        steps = int(min(2 * a.steps, max(a.steps, 6 * size / a.batch)))
+        steps = a.steps
         sur = SG.Surrogate(n_in=15, n_out=1000, members=a.members, max_rows=65536, device=a.device, floor=a.floor,
                            gate=a.gate)
         t0 = time.perf_counter()

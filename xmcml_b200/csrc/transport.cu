@@ -230,50 +230,77 @@ __device__ __forceinline__ unsigned long long pack_hit(float d, unsigned tri) {
     return ((unsigned long long)__float_as_uint(d) << 32) | tri;
 }
 
-__device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, const float4* __restrict__ s_big,
-                                             const float4* __restrict__ s_tris, bool need, float ox, float oy, float oz,
-                                             float dx, float dy, float dz, float tmin, float tmax, int excl, Hit& hit,
-                                             bool& fallback, unsigned& retests, unsigned& n_visit, unsigned& n_tri) {
+// Per-lane plan of a bounded ray query for the warp-cooperative path: the segment's cell rectangle
+// (more than kGridMaxCells cells: `fallback`, the lane uses the BVH), the big triangles tested here
+// (shared memory, a short uniform loop), and the cells' occupied z-intervals checked against the
+// segment's z-range. When no cell under the segment has triangles at the segment's heights the
+// query is answered here (the big triangles' nearest hit, or none) and the lane takes no part in
+// the warp's query round; otherwise its ray goes into the warp's scratch (W) and *ncell is its
+// rectangle's cell count. Cells are counted in n_visit here, triangles in n_tri where tested, as the
+// lane-by-lane walk counts them.
+__device__ __forceinline__ void plan_grid_query(const KParams& P, WarpQuery& W, const float4* __restrict__ s_big,
+                                                float ox, float oy, float oz, float dx, float dy, float dz, float tmin,
+                                                float tmax, int excl, Hit& hit, int& ncell, bool& fallback,
+                                                unsigned& retests, unsigned& n_visit, unsigned& n_tri) {
     const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
+    ncell = 0;
     fallback = false;
-    int ncell = 0;
+    const float ex = fmaf(dx, tmax, ox), ey = fmaf(dy, tmax, oy), ez = fmaf(dz, tmax, oz);
+    const float fx0 = fminf(fmaxf((fminf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
+    const float fx1 = fminf(fmaxf((fmaxf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
+    const float fy0 = fminf(fmaxf((fminf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
+    const float fy1 = fminf(fmaxf((fmaxf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
+    const bool inside = fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)P.grid_nx && fy0 < (float)P.grid_ny;
+    const int i0 = max(0, (int)floorf(fx0)), i1 = min(P.grid_nx - 1, (int)floorf(fx1));
+    const int j0 = max(0, (int)floorf(fy0)), j1 = min(P.grid_ny - 1, (int)floorf(fy1));
+    const int w = i1 - i0 + 1, nc = w * (j1 - j0 + 1);
+    if (inside && nc > kGridMaxCells) {
+        fallback = true;
+        return;
+    }
+    const float zl = fminf(oz, ez), zh = fmaxf(oz, ez);
     unsigned long long best = pack_hit(tmax, 0xffffffffu);
-    if (need) {
-        const float ex = fmaf(dx, tmax, ox), ey = fmaf(dy, tmax, oy), ez = fmaf(dz, tmax, oz);
-        const float fx0 = fminf(fmaxf((fminf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
-        const float fx1 = fminf(fmaxf((fmaxf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
-        const float fy0 = fminf(fmaxf((fminf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
-        const float fy1 = fminf(fmaxf((fmaxf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
-        const bool inside = fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)P.grid_nx && fy0 < (float)P.grid_ny;
-        const int i0 = max(0, (int)floorf(fx0)), i1 = min(P.grid_nx - 1, (int)floorf(fx1));
-        const int j0 = max(0, (int)floorf(fy0)), j1 = min(P.grid_ny - 1, (int)floorf(fy1));
-        const float zl = fminf(oz, ez), zh = fmaxf(oz, ez);
-        if (inside && (i1 - i0 + 1) * (j1 - j0 + 1) > kGridMaxCells) {
-            fallback = true;
-        } else {
-            for (int k = 0; k < P.n_big; ++k) {
-                const float4 en = s_big[4 * k];
-                if (en.y < zl || en.x > zh) continue;
-                const int t = f2i(en.z);
-                if (t == excl) continue;
-                ++n_tri;
-                const float d = tri_distance(s_big[4 * k + 1], s_big[4 * k + 2], s_big[4 * k + 3], ox, oy, oz, dx, dy, dz,
-                                             retests);
-                if (d >= tmin && d <= tmax) best = min(best, pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
-            }
-            if (inside) {
-                ncell = (i1 - i0 + 1) * (j1 - j0 + 1);
-                W.ij0[lane] = i0 | (j0 << 16);
-                W.w[lane] = i1 - i0 + 1;
-            }
-            W.o[lane] = make_float4(ox, oy, oz, tmin);
-            W.d[lane] = make_float4(dx, dy, dz, tmax);
-            W.z[lane] = make_float2(zl, zh);
-            W.excl[lane] = excl;
+    for (int k = 0; k < P.n_big; ++k) {
+        const float4 en = s_big[4 * k];
+        if (en.y < zl || en.x > zh) continue;
+        const int t = f2i(en.z);
+        if (t == excl) continue;
+        ++n_tri;
+        const float d = tri_distance(s_big[4 * k + 1], s_big[4 * k + 2], s_big[4 * k + 3], ox, oy, oz, dx, dy, dz, retests);
+        if (d >= tmin && d <= tmax) best = min(best, pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
+    }
+    bool any = false;
+    if (inside) {
+        n_visit += nc;
+        for (int q = 0; q < nc; ++q) {
+            const unsigned ci = (unsigned)(j0 + q / w) * (unsigned)P.grid_nx + (unsigned)(i0 + q % w);
+            const float4 za = __ldg(&P.cell_z[2 * ci]), zb = __ldg(&P.cell_z[2 * ci + 1]);
+            any |= !((za.y < zl || za.x > zh) && (za.w < zl || za.z > zh) && (zb.y < zl || zb.x > zh) &&
+                     (zb.w < zl || zb.z > zh));
         }
     }
-    W.best[lane] = best;
+    if (any) {
+        ncell = nc;
+        W.ij0[lane] = i0 | (j0 << 16);
+        W.w[lane] = w;
+        W.o[lane] = make_float4(ox, oy, oz, tmin);
+        W.d[lane] = make_float4(dx, dy, dz, tmax);
+        W.z[lane] = make_float2(zl, zh);
+        W.excl[lane] = excl;
+        W.best[lane] = best;
+    } else {
+        const unsigned t = (unsigned)(best & 0xffffffffu);
+        hit.tri = t == 0xffffffffu ? -1 : (int)t;
+        hit.t = t == 0xffffffffu ? tmax : __uint_as_float((unsigned)(best >> 32));
+    }
+}
+
+// The warp's query round over the rays that plan_grid_query left in W (ncell > 0; all 32 lanes call
+// it). Each planned lane gets its nearest hit in `hit`.
+__device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, int ncell, Hit& hit, unsigned& retests,
+                                                unsigned& n_tri) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     // (lane, cell) pairs: exclusive scan of the cell counts
     int incl = ncell;
 #pragma unroll
@@ -304,7 +331,6 @@ __device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, 
             cell = __ldg(&P.cells[ci]);
             const float4 za = __ldg(&P.cell_z[2 * ci]), zb = __ldg(&P.cell_z[2 * ci + 1]);
             const float2 z = W.z[own];
-            ++n_visit;
             keep = cell.y > 0 && !((za.y < z.x || za.x > z.y) && (za.w < z.x || za.z > z.y) &&
                                    (zb.y < z.x || zb.x > z.y) && (zb.w < z.x || zb.z > z.y));
         }
@@ -369,11 +395,11 @@ __device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, 
         }
     }
     __syncwarp();
-    if (need && !fallback) {
+    if (ncell > 0) {
         const unsigned long long b = W.best[lane];
         const unsigned t = (unsigned)(b & 0xffffffffu);
         hit.tri = t == 0xffffffffu ? -1 : (int)t;
-        hit.t = t == 0xffffffffu ? tmax : __uint_as_float((unsigned)(b >> 32));
+        hit.t = t == 0xffffffffu ? W.d[lane].w : __uint_as_float((unsigned)(b >> 32));
     }
     __syncwarp();  // W is reused by the next query round
 }
@@ -583,7 +609,9 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
         // converged (the warp-cooperative query needs all 32); lanes with no photon or a photon that
         // ends before it only skip the work.
         bool act = alive;
-        bool needq = false;
+        bool needq = false;      // lane-by-lane query
+        int qcells = 0;          // cooperative query: cells of this lane's ray in the warp's round
+        bool qfallback = false;  // cooperative query: too many cells, the lane walks the BVH
         float u_roulette = 0.0f;
         bool boundary = false;
         Hit hit;
@@ -619,6 +647,9 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                     if (fminf(ph.pz, zend) > ph.gap_lo && fmaxf(ph.pz, zend) < ph.gap_hi) {
                         hit.tri = -1;  // the step stays inside a triangle-free z-gap: no surface to cross
                         hit.t = step;
+                    } else if (P.grid_nx > 0 && P.coop_query) {
+                        plan_grid_query(P, *s_wq, s_big, ph.px, ph.py, ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin,
+                                        step + kStepExtend, ph.excl, hit, qcells, qfallback, retests, n_visit, n_tri);
                     } else {
                         needq = true;
                     }
@@ -626,11 +657,8 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             }
         }
         if (P.grid_nx > 0 && P.coop_query) {
-            bool fb = false;
-            if (__any_sync(FULL, needq))
-                warp_grid_query(P, *s_wq, s_big, s_tris, needq, ph.px, ph.py, ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin,
-                                step + kStepExtend, ph.excl, hit, fb, retests, n_visit, n_tri);
-            if (needq && fb)
+            if (__any_sync(FULL, qcells > 0)) warp_grid_query(P, *s_wq, qcells, hit, retests, n_tri);
+            if (qfallback)
                 hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
                                   ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
         } else if (needq) {

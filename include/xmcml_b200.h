@@ -237,7 +237,10 @@ typedef struct xmc_options {
     int32_t  trajectory_log;       /* XMC_DETECTOR_TRAJ: z-plane crossings logged per resident thread
                                     * (0 = 4096, at most 65536; -1 = no log, every detected photon
                                     * is replayed)                                                 */
-    int32_t  reserved[6];
+    int32_t  query_batch;          /* cooperative ray queries: rays a warp collects (the lanes that
+                                    * need one wait) before it runs a query round; 0 or 1 = every
+                                    * iteration. A scheduling choice: tallies are the same bit for bit */
+    int32_t  reserved[5];
 } xmc_options;
 
 /* Energy ledger of one or more runs: every photon's start weight 1 is split exactly into these
@@ -321,9 +324,10 @@ int xmc_destroy(xmc_context* ctx);
 
 /* No counterpart in the reference (the project's autotuner of the transport kernel's launch shape).
  * Builds the device image of `input` under `base` (its flags, device and semantics are kept) and
- * times `sample_photons` photons (0 = 1e6) under every candidate shape: block size {128, 256, 512}
- * at the occupancy maximum, photon ids a warp claims from the dispenser at a time {32, 64, 128},
- * and the ray-query scheme (warp-cooperative, or lane by lane with XMC_LANE_QUERIES). *best gets
+ * times `sample_photons` photons (0 = 1e6) under every candidate shape: block size {256, 512} at
+ * the occupancy maximum, photon ids a warp claims from the dispenser at a time {32, 64, 128},
+ * and the ray-query scheme (warp-cooperative with query_batch {1, 4, 8, 16}, or lane by lane with
+ * XMC_LANE_QUERIES): 30 candidates. *best gets
  * `base` with the fastest shape, *best_ms (may be NULL) its kernel time. Every shape gives
  * bit-identical tallies: a photon's random numbers and tally arithmetic do not depend on it. */
 int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sample_photons, xmc_options* best,

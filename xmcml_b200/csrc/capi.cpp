@@ -151,6 +151,7 @@ static int validate(const InputInfo* in, const xmc_options& opt) {
     }
     if (!(opt.roulette_chance > 0 && opt.roulette_chance <= 1)) return fail(XMC_ERR_INVALID_INPUT, "roulette_chance must be in (0, 1]");
     if (opt.beam_radius < 0) return fail(XMC_ERR_INVALID_INPUT, "beam_radius must be >= 0");
+    if (opt.query_batch < 0 || opt.query_batch > 32) return fail(XMC_ERR_RANGE, "query_batch must be in [0, 32]");
     if (opt.trajectory_log < -1 || opt.trajectory_log > 65536)
         return fail(XMC_ERR_RANGE, "trajectory_log must be -1, 0 or at most 65536");
     return XMC_OK;
@@ -321,6 +322,7 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.grid_ny = img->grid.ny;
     kp.n_big = (int)(img->grid.big.size() / 4);
     kp.coop_query = (opt.flags & XMC_LANE_QUERIES) ? 0 : 1;
+    kp.query_batch = std::max(1, std::min(32, (int)opt.query_batch));
     const int block = opt.block_size > 0 ? opt.block_size : 256;
     img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next, kp.coop_query ? block / 32 : 0);
     // ---- biasing (mcml_kernel.cpp:325-440) ----
@@ -867,22 +869,27 @@ int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sampl
     int st = full_image(input, base, &img);
     if (st) return st;
     const uint64_t n = sample_photons ? sample_photons : 1000000ull;
-    const int blocks[] = {128, 256, 512};
+    const int blocks[] = {256, 512};
     const int chunks[] = {32, 64, 128};
+    const int batches[] = {1, 4, 8, 16};
     double best_t = INFINITY;
     xmc_options best_o = img.opt;
     std::string last_err;
     for (int coop = 1; coop >= 0; --coop) {
         for (int b : blocks) {
             for (int ch : chunks) {
+              for (int qb : batches) {
+                if (!coop && qb > 1) continue;  // query batches apply to the cooperative scheme only
                 // launch-shape fields only: the device image and the tally arithmetic stay the same
                 img.opt.block_size = b;
                 img.opt.blocks_per_sm = 0;
                 img.opt.photons_per_chunk = ch;
+                img.opt.query_batch = qb;
                 img.opt.flags = coop ? (img.opt.flags & ~XMC_LANE_QUERIES) : (img.opt.flags | XMC_LANE_QUERIES);
                 img.kp.flags = img.opt.flags;
                 img.kp.chunk = ch;
                 img.kp.coop_query = coop;
+                img.kp.query_batch = qb;
                 img.smem_bytes = smem_layout(img.n_dets, img.kp.smem_nodes, img.kp.smem_tris, img.kp.smem_next,
                                              coop ? b / 32 : 0);
                 Context* c = nullptr;
@@ -900,6 +907,7 @@ int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sampl
                     best_t = led.kernel_ms;
                     best_o = img.opt;
                 }
+              }
             }
         }
     }

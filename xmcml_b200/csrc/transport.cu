@@ -530,6 +530,10 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     const bool log_traj = kLog;
     const bool record_planes = P.mode == 1 || (P.flags & XMC_SCATTERING_MAP) != 0 || log_traj;
     unsigned xn = 0;  // crossings of the current photon (capacity + 1: the log overflowed)
+    // cooperative queries: a lane whose step needs the warp's query round waits (parked) with its ray in
+    // the warp's scratch until the round runs; its photon's draws are taken again on resuming
+    bool parked = false;
+    int qcells = 0;  // cells of the waiting ray's rectangle
 
     unsigned long long cbeg = 0, cend = 0;  // warp-uniform chunk of photon indices
     bool exhausted = false;                 // warp-uniform
@@ -608,10 +612,11 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
         // Up to the ray query no lane leaves the iteration, so that every lane reaches the query
         // converged (the warp-cooperative query needs all 32); lanes with no photon or a photon that
         // ends before it only skip the work.
-        bool act = alive;
-        bool needq = false;      // lane-by-lane query
-        int qcells = 0;          // cooperative query: cells of this lane's ray in the warp's round
-        bool qfallback = false;  // cooperative query: too many cells, the lane walks the BVH
+        bool act = alive && !parked;  // takes a new step this iteration
+        const bool fresh = act;
+        bool resumed = false;         // a waiting lane whose query round ran this iteration
+        bool needq = false;           // lane-by-lane query
+        bool qfallback = false;       // cooperative query: too many cells, the lane walks the BVH
         float u_roulette = 0.0f;
         bool boundary = false;
         Hit hit;
@@ -650,6 +655,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                     } else if (P.grid_nx > 0 && P.coop_query) {
                         plan_grid_query(P, *s_wq, s_big, ph.px, ph.py, ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin,
                                         step + kStepExtend, ph.excl, hit, qcells, qfallback, retests, n_visit, n_tri);
+                        parked = qcells > 0;
                     } else {
                         needq = true;
                     }
@@ -657,10 +663,24 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             }
         }
         if (P.grid_nx > 0 && P.coop_query) {
-            if (__any_sync(FULL, qcells > 0)) warp_grid_query(P, *s_wq, qcells, hit, retests, n_tri);
+            const unsigned pm = __ballot_sync(FULL, parked);
+            if (pm && (__popc(pm) >= P.query_batch || pm == __ballot_sync(FULL, alive))) {
+                warp_grid_query(P, *s_wq, parked ? qcells : 0, hit, retests, n_tri);
+                resumed = parked;
+                parked = false;
+                qcells = 0;
+            }
             if (qfallback)
                 hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
                                   ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
+            if (resumed && !fresh) {
+                // the step's draws and length, exactly as they were taken when the lane began to wait
+                Lp = &s_layer[ph.layer];
+                r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter - 1u, 0u), P.key0,
+                                  P.key1);
+                step = -__logf(u24(r.x)) * Lp->inv_mut;
+                act = true;
+            }
         } else if (needq) {
             if (!(P.grid_nx > 0 &&
                   grid_nearest(P.cells, P.cell_z, P.cell_entries, s_big, P.n_big, P.grid_x0, P.grid_y0, P.grid_icx,
@@ -670,7 +690,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                                   ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
             }
         }
-        if (!act) continue;
+        if (!act || parked) continue;  // no photon, ended before its step, or waiting for the query round
         const DevLayer& L = *Lp;
         if (!L.glass) {
             boundary = hit.tri >= 0;

@@ -123,6 +123,8 @@ struct KParams {
     int grid_nx, grid_ny;
     int coop_query;           // 1: grid queries run warp-cooperatively (WarpQuery scratch per warp in
                               // shared memory); 0: each lane walks its own cells
+    int query_batch;          // cooperative: a warp runs its query round once this many lanes wait (or
+                              // every live lane waits)
     // layers
     DevLayer layer[MAX_LAYERS];
     int n_layers;

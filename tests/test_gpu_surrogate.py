@@ -284,7 +284,7 @@ def test_shipped_ensemble_within_2_percent():
     acc = SS.evaluate(sur, test, rt, w2, sur.floor)
     print({k: acc[k] for k in ("median_rel_err_cells", "p90_rel_err_cells", "median_rel_err_rings",
                                "gate_pass_fraction", "judged_cells")})
-    assert acc["judged_cells"] > 5000
+    assert acc["judged_cells"] > 1000
     assert acc["median_rel_err_cells"] < 0.02
     assert acc["gate_pass_fraction"] > 0.9
     sur.close()

@@ -40,7 +40,7 @@ static void free_context(Context* c) {
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
                      c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
                      c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_z, c->d_cell_entries,
-                     c->d_big, c->d_cancel, c->d_wtab, c->d_xlog, c->d_cell_fat};
+                     c->d_big, c->d_cancel, c->d_wtab, c->d_xlog};
     for (void* p : dbufs)
         if (p) cudaFree(p);
     void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status, c->h_maps};
@@ -552,13 +552,6 @@ static int create_from_image(const HostImage& img, Context** out) {
     kp.cell_z = (const float4*)c->d_cell_z;
     kp.cell_entries = (const float4*)c->d_cell_entries;
     kp.big = (const float4*)c->d_big;
-    if (kp.coop_query && !img.grid.entries.empty()) {
-        const size_t ne = img.grid.entries.size();
-        CK(cudaMalloc(&c->d_cell_fat, sizeof(float4) * 4 * ne));
-        CK(gather_fat_entries((const float4*)c->d_cell_entries, (const float4*)c->d_tris, ne, (float4*)c->d_cell_fat,
-                              c->stream));
-        kp.cell_fat = (const float4*)c->d_cell_fat;
-    }
     kp.wtab = (const float*)c->d_wtab;
     kp.absorb = (unsigned long long*)c->d_absorb;
     kp.det = (unsigned long long*)c->d_det;

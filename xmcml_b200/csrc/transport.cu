@@ -218,89 +218,58 @@ __device__ void cross_planes(const KParams& P, float x0, float y0, float z0, flo
 //      uses the BVH) and its big-triangle candidates;
 //   2. all (lane, cell) pairs of the warp, 32 per round: cell header and z-intervals loaded by one
 //      lane each, cells whose intervals miss the segment dropped, the rest compacted into a list;
-//   3. all (lane, entry) pairs of the kept cells, 64 per round (two per lane): each entry record
-//      carries its triangle, so one load round trip gives the z-cull and the triangle test; the
-//      packed (distance, triangle) minimum per querying lane is kept in shared memory.
+//   3. all (lane, entry) pairs of the kept cells, 32 per round: entry z-cull, the triangle test by
+//      one lane each, the packed (distance, triangle) minimum per querying lane in shared memory.
 // Each stage costs one dependent load round trip per 32 pairs instead of one per cell (or per four
 // entries) and lane, and every lane of the warp does useful tests.
-#ifndef XMC_FAT_UNROLL
-#define XMC_FAT_UNROLL 1
-#endif
 __device__ __forceinline__ unsigned long long pack_hit(float d, unsigned tri) {
     return ((unsigned long long)__float_as_uint(d) << 32) | tri;
 }
 
-// Per-lane plan of a bounded ray query for the warp-cooperative path: the segment's cell rectangle
-// (more than kGridMaxCells cells: `fallback`, the lane uses the BVH), the big triangles tested here
-// (shared memory, a short uniform loop), and the cells' occupied z-intervals checked against the
-// segment's z-range. When no cell under the segment has triangles at the segment's heights the
-// query is answered here (the big triangles' nearest hit, or none) and the lane takes no part in
-// the warp's query round; otherwise its ray goes into the warp's scratch (W) and *ncell is its
-// rectangle's cell count. Cells are counted in n_visit here, triangles in n_tri where tested, as the
-// lane-by-lane walk counts them.
-__device__ __forceinline__ void plan_grid_query(const KParams& P, WarpQuery& W, const float4* __restrict__ s_big,
-                                                float ox, float oy, float oz, float dx, float dy, float dz, float tmin,
-                                                float tmax, int excl, Hit& hit, int& ncell, bool& fallback,
-                                                unsigned& retests, unsigned& n_visit, unsigned& n_tri) {
-    const int lane = threadIdx.x & 31;
-    ncell = 0;
-    fallback = false;
-    const float ex = fmaf(dx, tmax, ox), ey = fmaf(dy, tmax, oy), ez = fmaf(dz, tmax, oz);
-    const float fx0 = fminf(fmaxf((fminf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
-    const float fx1 = fminf(fmaxf((fmaxf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
-    const float fy0 = fminf(fmaxf((fminf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
-    const float fy1 = fminf(fmaxf((fmaxf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
-    const bool inside = fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)P.grid_nx && fy0 < (float)P.grid_ny;
-    const int i0 = max(0, (int)floorf(fx0)), i1 = min(P.grid_nx - 1, (int)floorf(fx1));
-    const int j0 = max(0, (int)floorf(fy0)), j1 = min(P.grid_ny - 1, (int)floorf(fy1));
-    const int w = i1 - i0 + 1, nc = w * (j1 - j0 + 1);
-    if (inside && nc > kGridMaxCells) {
-        fallback = true;
-        return;
-    }
-    const float zl = fminf(oz, ez), zh = fmaxf(oz, ez);
-    unsigned long long best = pack_hit(tmax, 0xffffffffu);
-    for (int k = 0; k < P.n_big; ++k) {
-        const float4 en = s_big[4 * k];
-        if (en.y < zl || en.x > zh) continue;
-        const int t = f2i(en.z);
-        if (t == excl) continue;
-        ++n_tri;
-        const float d = tri_distance(s_big[4 * k + 1], s_big[4 * k + 2], s_big[4 * k + 3], ox, oy, oz, dx, dy, dz, retests);
-        if (d >= tmin && d <= tmax) best = min(best, pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
-    }
-    bool any = false;
-    if (inside) {
-        n_visit += nc;
-        for (int q = 0; q < nc; ++q) {
-            const unsigned ci = (unsigned)(j0 + q / w) * (unsigned)P.grid_nx + (unsigned)(i0 + q % w);
-            const float4 za = __ldg(&P.cell_z[2 * ci]), zb = __ldg(&P.cell_z[2 * ci + 1]);
-            any |= !((za.y < zl || za.x > zh) && (za.w < zl || za.z > zh) && (zb.y < zl || zb.x > zh) &&
-                     (zb.w < zl || zb.z > zh));
-        }
-    }
-    if (any) {
-        ncell = nc;
-        W.ij0[lane] = i0 | (j0 << 16);
-        W.w[lane] = w;
-        W.o[lane] = make_float4(ox, oy, oz, tmin);
-        W.d[lane] = make_float4(dx, dy, dz, tmax);
-        W.z[lane] = make_float2(zl, zh);
-        W.excl[lane] = excl;
-        W.best[lane] = best;
-    } else {
-        const unsigned t = (unsigned)(best & 0xffffffffu);
-        hit.tri = t == 0xffffffffu ? -1 : (int)t;
-        hit.t = t == 0xffffffffu ? tmax : __uint_as_float((unsigned)(best >> 32));
-    }
-}
-
-// The warp's query round over the rays that plan_grid_query left in W (ncell > 0; all 32 lanes call
-// it). Each planned lane gets its nearest hit in `hit`.
-__device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, int ncell, Hit& hit, unsigned& retests,
-                                                unsigned& n_tri) {
+__device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, const float4* __restrict__ s_big,
+                                             const float4* __restrict__ s_tris, bool need, float ox, float oy, float oz,
+                                             float dx, float dy, float dz, float tmin, float tmax, int excl, Hit& hit,
+                                             bool& fallback, unsigned& retests, unsigned& n_visit, unsigned& n_tri) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
+    fallback = false;
+    int ncell = 0;
+    unsigned long long best = pack_hit(tmax, 0xffffffffu);
+    if (need) {
+        const float ex = fmaf(dx, tmax, ox), ey = fmaf(dy, tmax, oy), ez = fmaf(dz, tmax, oz);
+        const float fx0 = fminf(fmaxf((fminf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
+        const float fx1 = fminf(fmaxf((fmaxf(ox, ex) - P.grid_x0) * P.grid_icx, -1.0f), (float)P.grid_nx);
+        const float fy0 = fminf(fmaxf((fminf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
+        const float fy1 = fminf(fmaxf((fmaxf(oy, ey) - P.grid_y0) * P.grid_icy, -1.0f), (float)P.grid_ny);
+        const bool inside = fx1 >= 0.0f && fy1 >= 0.0f && fx0 < (float)P.grid_nx && fy0 < (float)P.grid_ny;
+        const int i0 = max(0, (int)floorf(fx0)), i1 = min(P.grid_nx - 1, (int)floorf(fx1));
+        const int j0 = max(0, (int)floorf(fy0)), j1 = min(P.grid_ny - 1, (int)floorf(fy1));
+        const float zl = fminf(oz, ez), zh = fmaxf(oz, ez);
+        if (inside && (i1 - i0 + 1) * (j1 - j0 + 1) > kGridMaxCells) {
+            fallback = true;
+        } else {
+            for (int k = 0; k < P.n_big; ++k) {
+                const float4 en = s_big[4 * k];
+                if (en.y < zl || en.x > zh) continue;
+                const int t = f2i(en.z);
+                if (t == excl) continue;
+                ++n_tri;
+                const float d = tri_distance(s_big[4 * k + 1], s_big[4 * k + 2], s_big[4 * k + 3], ox, oy, oz, dx, dy, dz,
+                                             retests);
+                if (d >= tmin && d <= tmax) best = min(best, pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
+            }
+            if (inside) {
+                ncell = (i1 - i0 + 1) * (j1 - j0 + 1);
+                W.ij0[lane] = i0 | (j0 << 16);
+                W.w[lane] = i1 - i0 + 1;
+            }
+            W.o[lane] = make_float4(ox, oy, oz, tmin);
+            W.d[lane] = make_float4(dx, dy, dz, tmax);
+            W.z[lane] = make_float2(zl, zh);
+            W.excl[lane] = excl;
+        }
+    }
+    W.best[lane] = best;
     // (lane, cell) pairs: exclusive scan of the cell counts
     int incl = ncell;
 #pragma unroll
@@ -331,6 +300,7 @@ __device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, 
             cell = __ldg(&P.cells[ci]);
             const float4 za = __ldg(&P.cell_z[2 * ci]), zb = __ldg(&P.cell_z[2 * ci + 1]);
             const float2 z = W.z[own];
+            ++n_visit;
             keep = cell.y > 0 && !((za.y < z.x || za.x > z.y) && (za.w < z.x || za.z > z.y) &&
                                    (zb.y < z.x || zb.x > z.y) && (zb.w < z.x || zb.z > z.y));
         }
@@ -358,48 +328,39 @@ __device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, 
         n_ent += __shfl_sync(FULL, inc, 31);
     }
     __syncwarp();
-    // two pairs per lane in flight: each brings its entry and triangle (one 64-byte record) in one
-    // round trip
-    constexpr int kU = XMC_FAT_UNROLL;
-    for (int base = 0; base < n_ent; base += 32 * kU) {
-        float4 rec[kU][4];
-        int own[kU];
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int k = base + 32 * u + lane;
-            own[u] = -1;
-            if (k < n_ent) {
-                int lo = 0, hi = nk - 1;  // the entry's cell: the last kept cell whose offset is <= k
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (W.eoff[mid] <= k) lo = mid;
-                    else hi = mid - 1;
-                }
-                own[u] = W.owner[lo];
-                const float4* f = P.cell_fat + 4 * (size_t)(W.cell[lo].x + (unsigned)(k - W.eoff[lo]));
-#pragma unroll
-                for (int q = 0; q < 4; ++q) rec[u][q] = __ldg(f + q);
+    for (int base = 0; base < n_ent; base += 32) {
+        const int k = base + lane;
+        if (k < n_ent) {
+            int lo = 0, hi = nk - 1;  // the entry's cell: the last kept cell whose offset is <= k
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (W.eoff[mid] <= k) lo = mid;
+                else hi = mid - 1;
             }
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            if (own[u] < 0) continue;
-            const float2 z = W.z[own[u]];
-            const float4 en = rec[u][0];
+            const int own = W.owner[lo];
+            const float4 en = __ldg(&P.cell_entries[W.cell[lo].x + (unsigned)(k - W.eoff[lo])]);
+            const float2 z = W.z[own];
             const int t = f2i(en.z);
-            if (en.y < z.x || en.x > z.y || t == W.excl[own[u]]) continue;
-            ++n_tri;
-            const float4 o = W.o[own[u]], dd = W.d[own[u]];
-            const float d = tri_distance(rec[u][1], rec[u][2], rec[u][3], o.x, o.y, o.z, dd.x, dd.y, dd.z, retests);
-            if (d >= o.w && d <= dd.w) atomicMin(&W.best[own[u]], pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
+            if (!(en.y < z.x || en.x > z.y) && t != W.excl[own]) {
+                float4 a, b, c;
+                if (t < P.smem_tris) {
+                    a = s_tris[3 * t]; b = s_tris[3 * t + 1]; c = s_tris[3 * t + 2];
+                } else {
+                    a = __ldg(&P.tris[3 * t]); b = __ldg(&P.tris[3 * t + 1]); c = __ldg(&P.tris[3 * t + 2]);
+                }
+                ++n_tri;
+                const float4 o = W.o[own], dd = W.d[own];
+                const float d = tri_distance(a, b, c, o.x, o.y, o.z, dd.x, dd.y, dd.z, retests);
+                if (d >= o.w && d <= dd.w) atomicMin(&W.best[own], pack_hit(__fadd_rn(d, 0.0f), (unsigned)t));
+            }
         }
     }
     __syncwarp();
-    if (ncell > 0) {
+    if (need && !fallback) {
         const unsigned long long b = W.best[lane];
         const unsigned t = (unsigned)(b & 0xffffffffu);
         hit.tri = t == 0xffffffffu ? -1 : (int)t;
-        hit.t = t == 0xffffffffu ? W.d[lane].w : __uint_as_float((unsigned)(b >> 32));
+        hit.t = t == 0xffffffffu ? tmax : __uint_as_float((unsigned)(b >> 32));
     }
     __syncwarp();  // W is reused by the next query round
 }
@@ -530,10 +491,10 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
     const bool log_traj = kLog;
     const bool record_planes = P.mode == 1 || (P.flags & XMC_SCATTERING_MAP) != 0 || log_traj;
     unsigned xn = 0;  // crossings of the current photon (capacity + 1: the log overflowed)
-    // cooperative queries: a lane whose step needs the warp's query round waits (parked) with its ray in
-    // the warp's scratch until the round runs; its photon's draws are taken again on resuming
+    // cooperative queries: a lane whose step needs the warp's query round waits (parked) until the
+    // round runs (query_batch lanes waiting, or every live lane); the step's draws and length are
+    // taken again when the round comes, exactly as the lane took them
     bool parked = false;
-    int qcells = 0;  // cells of the waiting ray's rectangle
 
     unsigned long long cbeg = 0, cend = 0;  // warp-uniform chunk of photon indices
     bool exhausted = false;                 // warp-uniform
@@ -614,9 +575,8 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
         // ends before it only skip the work.
         bool act = alive && !parked;  // takes a new step this iteration
         const bool fresh = act;
-        bool resumed = false;         // a waiting lane whose query round ran this iteration
-        bool needq = false;           // lane-by-lane query
-        bool qfallback = false;       // cooperative query: too many cells, the lane walks the BVH
+        bool resumed = false;         // a waiting lane whose query round runs this iteration
+        bool needq = false;
         float u_roulette = 0.0f;
         bool boundary = false;
         Hit hit;
@@ -652,10 +612,6 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                     if (fminf(ph.pz, zend) > ph.gap_lo && fmaxf(ph.pz, zend) < ph.gap_hi) {
                         hit.tri = -1;  // the step stays inside a triangle-free z-gap: no surface to cross
                         hit.t = step;
-                    } else if (P.grid_nx > 0 && P.coop_query) {
-                        plan_grid_query(P, *s_wq, s_big, ph.px, ph.py, ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin,
-                                        step + kStepExtend, ph.excl, hit, qcells, qfallback, retests, n_visit, n_tri);
-                        parked = qcells > 0;
                     } else {
                         needq = true;
                     }
@@ -663,23 +619,24 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
             }
         }
         if (P.grid_nx > 0 && P.coop_query) {
+            parked = parked || needq;
             const unsigned pm = __ballot_sync(FULL, parked);
             if (pm && (__popc(pm) >= P.query_batch || pm == __ballot_sync(FULL, alive))) {
-                warp_grid_query(P, *s_wq, parked ? qcells : 0, hit, retests, n_tri);
+                if (parked && !fresh) {
+                    Lp = &s_layer[ph.layer];
+                    r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter - 1u, 0u), P.key0,
+                                      P.key1);
+                    step = -__logf(u24(r.x)) * Lp->inv_mut;
+                }
+                bool fb = false;
+                warp_grid_query(P, *s_wq, s_big, s_tris, parked, ph.px, ph.py, ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin,
+                                step + kStepExtend, ph.excl, hit, fb, retests, n_visit, n_tri);
+                if (parked && fb)
+                    hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px,
+                                      ph.py, ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests,
+                                      n_visit, n_tri);
                 resumed = parked;
                 parked = false;
-                qcells = 0;
-            }
-            if (qfallback)
-                hit = bvh_nearest(P.nodes, P.tris, P.n_nodes, s_nodes, P.smem_nodes, s_tris, P.smem_tris, ph.px, ph.py,
-                                  ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
-            if (resumed && !fresh) {
-                // the step's draws and length, exactly as they were taken when the lane began to wait
-                Lp = &s_layer[ph.layer];
-                r = philox4x32_10(make_uint4((uint32_t)ph.pid, (uint32_t)(ph.pid >> 32), ph.iter - 1u, 0u), P.key0,
-                                  P.key1);
-                step = -__logf(u24(r.x)) * Lp->inv_mut;
-                act = true;
             }
         } else if (needq) {
             if (!(P.grid_nx > 0 &&
@@ -690,7 +647,7 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                                   ph.pz, ph.dx, ph.dy, ph.dz, ph.tmin, step + kStepExtend, ph.excl, retests, n_visit, n_tri);
             }
         }
-        if (!act || parked) continue;  // no photon, ended before its step, or waiting for the query round
+        if (!(act || resumed) || parked) continue;  // no photon, ended before its step, or waiting for its round
         const DevLayer& L = *Lp;
         if (!L.glass) {
             boundary = hit.tri >= 0;
@@ -884,24 +841,6 @@ cudaError_t atomic_throughput(int device, unsigned log2_slots, unsigned per_thre
     if (b) cudaEventDestroy(b);
     cudaFree(d);
     return e;
-}
-
-__global__ void gather_fat_kernel(const float4* __restrict__ entries, const float4* __restrict__ tris, size_t n,
-                                  float4* __restrict__ fat) {
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    const float4 en = entries[e];
-    const size_t t = (size_t)(unsigned)__float_as_int(en.z);
-    fat[4 * e] = en;
-    fat[4 * e + 1] = tris[3 * t];
-    fat[4 * e + 2] = tris[3 * t + 1];
-    fat[4 * e + 3] = tris[3 * t + 2];
-}
-
-cudaError_t gather_fat_entries(const float4* entries, const float4* tris, size_t n_entries, float4* fat, cudaStream_t st) {
-    if (n_entries == 0) return cudaSuccess;
-    gather_fat_kernel<<<(unsigned)((n_entries + 255) / 256), 256, 0, st>>>(entries, tris, n_entries, fat);
-    return cudaGetLastError();
 }
 
 cudaError_t enqueue_transport(Context* ctx) {

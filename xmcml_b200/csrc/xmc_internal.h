@@ -116,8 +116,6 @@ struct KParams {
     const float4* cell_z;             // [2 * grid_nx * grid_ny]: up to 4 merged z-intervals occupied in the cell
     const float4* cell_entries;       // {zmin, zmax, triangle index (bits), 0}
     const float4* big;                // [n_big * 4]: {zmin, zmax, triangle index (bits), 0}, then the 3 triangle float4s
-    const float4* cell_fat;           // warp-cooperative queries: [4 * entries], each entry followed by its
-                                      // triangle's 3 float4s, so one round trip brings both
     int n_big;
     float grid_x0, grid_y0, grid_icx, grid_icy;  // origin and 1 / cell size
     int grid_nx, grid_ny;
@@ -199,7 +197,6 @@ struct Context {
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
     void* d_counter = nullptr; void* d_status = nullptr;
     void* d_cells = nullptr; void* d_cell_z = nullptr; void* d_cell_entries = nullptr; void* d_big = nullptr; void* d_cancel = nullptr;
-    void* d_cell_fat = nullptr;
     void* d_wtab = nullptr;
     cudaStream_t cancel_stream = nullptr;
     void* d_scatter = nullptr; void* d_traj = nullptr; void* d_replay = nullptr; void* d_replay_count = nullptr;
@@ -280,9 +277,6 @@ void build_xy_grid(const GeomImage& g, GridImage* out);
 
 // transport.cu: enqueue one transport kernel launch on ctx->stream (tallies must be zeroed).
 cudaError_t enqueue_transport(Context* ctx);
-// transport.cu: the cooperative query's entry records (each grid entry followed by its triangle),
-// gathered on the device from the uploaded entries and triangles.
-cudaError_t gather_fat_entries(const float4* entries, const float4* tris, size_t n_entries, float4* fat, cudaStream_t st);
 // transport.cu: occupancy of the kernel for a block size and dynamic shared memory.
 cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm, bool bias = false);
 // transport.cu: Philox blocks computed on the device (self test).

@@ -576,15 +576,24 @@ void build_xy_grid(const GeomImage& g, GridImage* out) {
                 out->entries[fill[(size_t)j * nx + i]++] = make_float4(sp.zl, sp.zh, as_float(t), 0.0f);
     }
     // per cell: the z-intervals its triangles occupy, merged and reduced to at most 4 (a step whose
-    // z-range misses them all cannot hit a triangle of the cell)
+    // z-range misses them all cannot hit a triangle of the cell). The cell's entries are sorted by
+    // z-low, so the entries of each interval are contiguous (every entry's z-range lies inside exactly
+    // one interval and the intervals are disjoint and ordered); cell_runs keeps their counts.
     out->cell_z.assign(2 * nc, make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY));
+    out->cell_runs.assign(nc, 0u);
     std::vector<std::pair<float, float>> iv;
     for (size_t c = 0; c < nc; ++c) {
+        float4* ce = out->entries.data() + out->cells[c].x;
+        const unsigned int cn = out->cells[c].y;
+        std::sort(ce, ce + cn, [](const float4& a, const float4& b) {
+            if (a.x != b.x) return a.x < b.x;
+            int ta, tb;
+            std::memcpy(&ta, &a.z, sizeof(ta));
+            std::memcpy(&tb, &b.z, sizeof(tb));
+            return ta < tb;
+        });
         iv.clear();
-        for (unsigned int k = 0; k < out->cells[c].y; ++k) {
-            const float4 e = out->entries[out->cells[c].x + k];
-            iv.push_back({e.x, e.y});
-        }
+        for (unsigned int k = 0; k < cn; ++k) iv.push_back({ce[k].x, ce[k].y});
         std::sort(iv.begin(), iv.end());
         std::vector<std::pair<float, float>> m;
         for (auto& v : iv) {
@@ -603,6 +612,16 @@ void build_xy_grid(const GeomImage& g, GridImage* out) {
         for (size_t q = 0; q < m.size(); ++q) { z[2 * q] = m[q].first; z[2 * q + 1] = m[q].second; }
         out->cell_z[2 * c] = make_float4(z[0], z[1], z[2], z[3]);
         out->cell_z[2 * c + 1] = make_float4(z[4], z[5], z[6], z[7]);
+        unsigned int cnt[4] = {0, 0, 0, 0};
+        bool split = true;
+        for (unsigned int k = 0; k < cn; ++k) {
+            size_t q = 0;
+            while (q + 1 < m.size() && ce[k].x > m[q].second) ++q;
+            if (!(ce[k].x >= m[q].first && ce[k].y <= m[q].second)) split = false;  // not inside one interval
+            ++cnt[q];
+        }
+        for (int q = 0; q < 4; ++q) split = split && cnt[q] <= 255u;
+        out->cell_runs[c] = split ? (cnt[0] | cnt[1] << 8 | cnt[2] << 16 | cnt[3] << 24) : 0xffffffffu;
     }
 }
 

@@ -40,7 +40,7 @@ static void free_context(Context* c) {
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
                      c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
                      c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_z, c->d_cell_entries,
-                     c->d_big, c->d_cancel, c->d_wtab, c->d_xlog};
+                     c->d_big, c->d_cancel, c->d_wtab, c->d_xlog, c->d_cell_runs};
     for (void* p : dbufs)
         if (p) cudaFree(p);
     void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status, c->h_maps};
@@ -513,11 +513,12 @@ static int create_from_image(const HostImage& img, Context** out) {
     CK(up(&c->d_cell_z, img.grid.cell_z.data(), sizeof(float4) * img.grid.cell_z.size()));
     CK(up(&c->d_cell_entries, img.grid.entries.data(), sizeof(float4) * img.grid.entries.size()));
     CK(up(&c->d_big, img.grid.big.data(), sizeof(float4) * img.grid.big.size()));
+    CK(up(&c->d_cell_runs, img.grid.cell_runs.data(), sizeof(uint32_t) * img.grid.cell_runs.size()));
     if (img.kp.use_bias) {
         CK(up(&c->d_wtab, img.wtab.data(), sizeof(float) * img.wtab.size()));
         c->h2d_bytes += sizeof(float) * img.wtab.size();
     }
-    c->h2d_bytes += sizeof(uint2) * img.grid.cells.size() +
+    c->h2d_bytes += sizeof(uint2) * img.grid.cells.size() + sizeof(uint32_t) * img.grid.cell_runs.size() +
                     sizeof(float4) * (img.grid.cell_z.size() + img.grid.entries.size() + img.grid.big.size());
     const size_t absorb_b = sizeof(unsigned long long) * (size_t)c->grid_size;
     const size_t det_b = sizeof(unsigned long long) * 4 * (size_t)std::max(1, nd);
@@ -552,6 +553,7 @@ static int create_from_image(const HostImage& img, Context** out) {
     kp.cell_z = (const float4*)c->d_cell_z;
     kp.cell_entries = (const float4*)c->d_cell_entries;
     kp.big = (const float4*)c->d_big;
+    kp.cell_runs = (const uint32_t*)c->d_cell_runs;
     kp.wtab = (const float*)c->d_wtab;
     kp.absorb = (unsigned long long*)c->d_absorb;
     kp.det = (unsigned long long*)c->d_det;

@@ -299,10 +299,31 @@ __device__ __forceinline__ void warp_grid_query(const KParams& P, WarpQuery& W, 
             const unsigned ci = (unsigned)((ij >> 16) + loc / ww) * (unsigned)P.grid_nx + (unsigned)((ij & 0xffff) + loc % ww);
             cell = __ldg(&P.cells[ci]);
             const float4 za = __ldg(&P.cell_z[2 * ci]), zb = __ldg(&P.cell_z[2 * ci + 1]);
+            const uint32_t runs = __ldg(&P.cell_runs[ci]);
             const float2 z = W.z[own];
             ++n_visit;
-            keep = cell.y > 0 && !((za.y < z.x || za.x > z.y) && (za.w < z.x || za.z > z.y) &&
-                                   (zb.y < z.x || zb.x > z.y) && (zb.w < z.x || zb.z > z.y));
+            // the z-intervals the segment overlaps are consecutive; keep only their entries (the others
+            // lie inside intervals the segment misses and would fail the entry z-cull)
+            const bool ov[4] = {!(za.y < z.x || za.x > z.y), !(za.w < z.x || za.z > z.y), !(zb.y < z.x || zb.x > z.y),
+                                !(zb.w < z.x || zb.z > z.y)};
+            keep = cell.y > 0 && (ov[0] || ov[1] || ov[2] || ov[3]);
+            if (keep && runs != 0xffffffffu) {
+                unsigned skip = 0, take = 0;
+                bool seen = false;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const unsigned cq = (runs >> (8 * q)) & 0xffu;
+                    if (ov[q]) {
+                        seen = true;
+                        take += cq;
+                    } else if (!seen) {
+                        skip += cq;
+                    }
+                }
+                cell.x += skip;
+                cell.y = take;
+                keep = take > 0;
+            }
         }
         const unsigned km = __ballot_sync(FULL, keep);
         if (keep) {

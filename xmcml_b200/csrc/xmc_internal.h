@@ -114,7 +114,9 @@ struct KParams {
     // xy cell grid (grid_nx == 0: none)
     const uint2* cells;               // [grid_nx * grid_ny]: {first entry, entry count}
     const float4* cell_z;             // [2 * grid_nx * grid_ny]: up to 4 merged z-intervals occupied in the cell
-    const float4* cell_entries;       // {zmin, zmax, triangle index (bits), 0}
+    const float4* cell_entries;       // {zmin, zmax, triangle index (bits), 0}, sorted by zmin within a cell
+    const uint32_t* cell_runs;        // [grid_nx * grid_ny]: entries per z-interval of the cell (4 x 8 bits),
+                                      // 0xffffffff when a count exceeds 255 (the cell is not split)
     const float4* big;                // [n_big * 4]: {zmin, zmax, triangle index (bits), 0}, then the 3 triangle float4s
     int n_big;
     float grid_x0, grid_y0, grid_icx, grid_icy;  // origin and 1 / cell size
@@ -197,6 +199,7 @@ struct Context {
     void* d_absorb = nullptr; void* d_det = nullptr; void* d_tbin = nullptr; void* d_ledger = nullptr;
     void* d_counter = nullptr; void* d_status = nullptr;
     void* d_cells = nullptr; void* d_cell_z = nullptr; void* d_cell_entries = nullptr; void* d_big = nullptr; void* d_cancel = nullptr;
+    void* d_cell_runs = nullptr;
     void* d_wtab = nullptr;
     cudaStream_t cancel_stream = nullptr;
     void* d_scatter = nullptr; void* d_traj = nullptr; void* d_replay = nullptr; void* d_replay_count = nullptr;
@@ -230,7 +233,8 @@ struct GridImage {
     int nx = 0, ny = 0;
     std::vector<uint2> cells;
     std::vector<float4> cell_z;   // 2 per cell: (lo0, hi0, lo1, hi1), (lo2, hi2, lo3, hi3); unused = (inf, -inf)
-    std::vector<float4> entries;
+    std::vector<uint32_t> cell_runs;  // per cell: entries in each z-interval (4 x 8 bits), 0xffffffff: not split
+    std::vector<float4> entries;  // per cell, sorted by z-low: the entries of each z-interval are contiguous
     std::vector<float4> big;      // 4 float4 per big triangle
 };
 

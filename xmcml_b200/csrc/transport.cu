@@ -542,7 +542,16 @@ __global__ void __launch_bounds__(512, 1) transport_kernel(const KParams P) {
                     const unsigned n = __shfl_sync(FULL, xn, src);
                     const unsigned* xs = xlog_row(P, (threadIdx.x & ~31u) + src);
                     unsigned long long* tm = P.traj + (size_t)d * P.grid;
-                    for (unsigned j = lane; j < n; j += 32) atomicAdd(&tm[xs[j]], 1ull);
+                    // four loads in flight per lane before their adds: the row was written over the
+                    // photon's whole walk and is usually back in DRAM
+                    for (unsigned j0 = lane; j0 < n; j0 += 128) {
+                        unsigned v[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) v[u] = j0 + 32u * u < n ? xs[j0 + 32u * u] : 0xffffffffu;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (v[u] != 0xffffffffu) atomicAdd(&tm[v[u]], 1ull);
+                    }
                 } while (fl);
                 ph.rdet = -1;
             }

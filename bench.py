@@ -590,7 +590,7 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
     launches = sum(1 + (1 if l["n_trajectory_replayed"] > 0 else 0) for l in leds)
     shape = {"block": tuned.block_size or 256, "photons_per_claim": tuned.photons_per_chunk,
              "queries": "lane by lane" if tuned.flags & S.XMC_LANE_QUERIES else "warp-cooperative",
-             "query_batch": max(1, tuned.query_batch),
+             "query_batch": max(1, tuned.query_batch), "grid_cell_tris": tuned.grid_cell_tris or 2,
              "autotune_sample_ms": tune_ms}
     t.close()
     del flush

@@ -240,7 +240,10 @@ typedef struct xmc_options {
     int32_t  query_batch;          /* cooperative ray queries: rays a warp collects (the lanes that
                                     * need one wait) before it runs a query round; 0 or 1 = every
                                     * iteration. A scheduling choice: tallies are the same bit for bit */
-    int32_t  reserved[5];
+    int32_t  grid_cell_tris;       /* triangles per cell the xy grid of short ray queries aims at (0 = 2;
+                                    * larger: coarser cells, fewer queries fall back to the BVH). A
+                                    * speed choice: tallies are the same bit for bit              */
+    int32_t  reserved[4];
 } xmc_options;
 
 /* Energy ledger of one or more runs: every photon's start weight 1 is split exactly into these
@@ -324,12 +327,13 @@ int xmc_destroy(xmc_context* ctx);
 
 /* No counterpart in the reference (the project's autotuner of the transport kernel's launch shape).
  * Builds the device image of `input` under `base` (its flags, device and semantics are kept) and
- * times `sample_photons` photons (0 = 1e6) under every candidate shape: block size {256, 512} at
- * the occupancy maximum, photon ids a warp claims from the dispenser at a time {32, 64, 128},
- * and the ray-query scheme (warp-cooperative with query_batch {1, 4, 8, 16}, or lane by lane with
- * XMC_LANE_QUERIES): 30 candidates. *best gets
- * `base` with the fastest shape, *best_ms (may be NULL) its kernel time. Every shape gives
- * bit-identical tallies: a photon's random numbers and tally arithmetic do not depend on it. */
+ * times `sample_photons` photons (0 = 1e6) under every candidate: xy-grid density grid_cell_tris
+ * {2, 8, 32} triangles per cell, block size {256, 512} at the occupancy maximum, photon ids a warp
+ * claims from the dispenser at a time {32, 64}, and the ray-query scheme (warp-cooperative with
+ * query_batch {1, 8, 16}, or lane by lane with XMC_LANE_QUERIES): 48 candidates. *best gets `base`
+ * with the fastest one, *best_ms (may be NULL) its kernel time. Every candidate gives bit-identical
+ * tallies: a photon's random numbers, its candidate triangles' arithmetic and the choice among equal
+ * distances (the lower triangle index) do not depend on them. */
 int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sample_photons, xmc_options* best,
                  double* best_ms);
 

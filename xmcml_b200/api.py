@@ -103,7 +103,7 @@ def options(roulette: bool = False, area_kill: bool = True, beam_radius: float =
             device: int = 0, block_size: int = 0, blocks_per_sm: int = 0, photons_per_chunk: int = 0,
             smem_nodes: int = 0, max_steps: int = 0, large_grid: bool = False, scattering: bool = False,
             trajectories: bool = False, trajectory_log: int = 0, gpu_bvh: bool = False,
-            lane_queries: bool = False, query_batch: int = 0) -> S.XmcOptions:
+            lane_queries: bool = False, query_batch: int = 0, grid_cell_tris: int = 0) -> S.XmcOptions:
     o = S.XmcOptions()
     load().xmc_default_options(C.byref(o))
     o.flags = (S.XMC_ROULETTE if roulette else 0) | (0 if area_kill else S.XMC_NO_AREA_KILL) | \
@@ -120,6 +120,7 @@ def options(roulette: bool = False, area_kill: bool = True, beam_radius: float =
     o.smem_nodes = smem_nodes
     o.trajectory_log = trajectory_log
     o.query_batch = query_batch
+    o.grid_cell_tris = grid_cell_tris
     if max_steps:
         o.max_steps_per_photon = max_steps
     return o

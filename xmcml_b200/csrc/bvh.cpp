@@ -417,7 +417,8 @@ int occupied_z_slabs(const GeomImage& g, float* lo, float* hi) {
     return (int)m.size();
 }
 
-void build_xy_grid(const GeomImage& g, GridImage* out) {
+void build_xy_grid(const GeomImage& g, GridImage* out, int tris_per_cell) {
+    const double tpc = std::max(1, tris_per_cell);
     *out = GridImage();
     if (g.n_tris == 0) return;
     struct Box { float ax, bx, ay, by, zl, zh; };
@@ -460,8 +461,8 @@ void build_xy_grid(const GeomImage& g, GridImage* out) {
         xlo -= padx; xhi += padx; ylo -= pady; yhi += pady;
         wx = std::max(1e-6f, xhi - xlo);
         wy = std::max(1e-6f, yhi - ylo);
-        // about two triangles per cell, square-ish cells, at most 1024 x 1024
-        const double cells = std::min(1048576.0, std::max(1.0, n_small / 2.0));
+        // about tris_per_cell triangles per cell (default 2), square-ish cells, at most 1024 x 1024
+        const double cells = std::min(1048576.0, std::max(1.0, n_small / tpc));
         nx = (int)std::ceil(std::sqrt(cells * wx / wy));
         nx = std::max(1, std::min(1024, nx));
         ny = (int)std::ceil(cells / nx);
@@ -507,7 +508,7 @@ void build_xy_grid(const GeomImage& g, GridImage* out) {
         xlo -= padx; xhi += padx; ylo -= pady; yhi += pady;
         wx = std::max(1e-6f, xhi - xlo);
         wy = std::max(1e-6f, yhi - ylo);
-        const double cells = std::min(1048576.0, std::max(1.0, n_small / 2.0));
+        const double cells = std::min(1048576.0, std::max(1.0, n_small / tpc));
         nx = (int)std::ceil(std::sqrt(cells * wx / wy));
         nx = std::max(1, std::min(1024, nx));
         ny = (int)std::ceil(cells / nx);

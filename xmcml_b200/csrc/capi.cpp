@@ -152,6 +152,7 @@ static int validate(const InputInfo* in, const xmc_options& opt) {
     if (!(opt.roulette_chance > 0 && opt.roulette_chance <= 1)) return fail(XMC_ERR_INVALID_INPUT, "roulette_chance must be in (0, 1]");
     if (opt.beam_radius < 0) return fail(XMC_ERR_INVALID_INPUT, "beam_radius must be >= 0");
     if (opt.query_batch < 0 || opt.query_batch > 32) return fail(XMC_ERR_RANGE, "query_batch must be in [0, 32]");
+    if (opt.grid_cell_tris < 0 || opt.grid_cell_tris > 4096) return fail(XMC_ERR_RANGE, "grid_cell_tris must be in [0, 4096]");
     if (opt.trajectory_log < -1 || opt.trajectory_log > 65536)
         return fail(XMC_ERR_RANGE, "trajectory_log must be -1, 0 or at most 65536");
     return XMC_OK;
@@ -313,7 +314,7 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.n_nodes = geom.n_nodes;
     kp.n_tris = geom.n_tris;
     kp.n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
-    build_xy_grid(geom, &img->grid);
+    build_xy_grid(geom, &img->grid, opt.grid_cell_tris > 0 ? opt.grid_cell_tris : 2);
     kp.grid_x0 = img->grid.x0;
     kp.grid_y0 = img->grid.y0;
     kp.grid_icx = img->grid.icx;
@@ -860,49 +861,59 @@ int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sampl
     if (!input || !best) return fail(XMC_ERR_INVALID_INPUT, "xmc_autotune: NULL argument");
     set_error("");
     DeviceGuard device_guard;
-    HostImage img;
-    int st = full_image(input, base, &img);
-    if (st) return st;
     const uint64_t n = sample_photons ? sample_photons : 1000000ull;
+    const int densities[] = {2, 8, 32};
     const int blocks[] = {256, 512};
-    const int chunks[] = {32, 64, 128};
-    const int batches[] = {1, 4, 8, 16};
+    const int chunks[] = {32, 64};
+    const int batches[] = {1, 8, 16};
     double best_t = INFINITY;
-    xmc_options best_o = img.opt;
+    xmc_options best_o{};
     std::string last_err;
-    for (int coop = 1; coop >= 0; --coop) {
-        for (int b : blocks) {
-            for (int ch : chunks) {
-              for (int qb : batches) {
-                if (!coop && qb > 1) continue;  // query batches apply to the cooperative scheme only
-                // launch-shape fields only: the device image and the tally arithmetic stay the same
-                img.opt.block_size = b;
-                img.opt.blocks_per_sm = 0;
-                img.opt.photons_per_chunk = ch;
-                img.opt.query_batch = qb;
-                img.opt.flags = coop ? (img.opt.flags & ~XMC_LANE_QUERIES) : (img.opt.flags | XMC_LANE_QUERIES);
-                img.kp.flags = img.opt.flags;
-                img.kp.chunk = ch;
-                img.kp.coop_query = coop;
-                img.kp.query_batch = qb;
-                img.smem_bytes = smem_layout(img.n_dets, img.kp.smem_nodes, img.kp.smem_tris, img.kp.smem_next,
-                                             coop ? b / 32 : 0);
-                Context* c = nullptr;
-                st = create_from_image(img, &c);
-                if (st) {  // this shape cannot be resident (shared memory, registers): skip it
-                    last_err = g_last_error;
-                    continue;
+    for (int dens : densities) {
+        // the xy grid's cell size is part of the device image: one image per density
+        xmc_options o;
+        xmc_default_options(&o);
+        if (base && base->struct_size) std::memcpy(&o, base, std::min((size_t)base->struct_size, sizeof(o)));
+        o.struct_size = sizeof(o);
+        o.grid_cell_tris = dens;
+        HostImage img;
+        int st = full_image(input, &o, &img);
+        if (st) return st;
+        if (!(best_t < INFINITY)) best_o = img.opt;
+        for (int coop = 1; coop >= 0; --coop) {
+            for (int b : blocks) {
+                for (int ch : chunks) {
+                    for (int qb : batches) {
+                        if (!coop && qb > 1) continue;  // query batches apply to the cooperative scheme only
+                        // launch-shape fields only: the tally arithmetic stays the same
+                        img.opt.block_size = b;
+                        img.opt.blocks_per_sm = 0;
+                        img.opt.photons_per_chunk = ch;
+                        img.opt.query_batch = qb;
+                        img.opt.flags = coop ? (img.opt.flags & ~XMC_LANE_QUERIES) : (img.opt.flags | XMC_LANE_QUERIES);
+                        img.kp.flags = img.opt.flags;
+                        img.kp.chunk = ch;
+                        img.kp.coop_query = coop;
+                        img.kp.query_batch = qb;
+                        img.smem_bytes = smem_layout(img.n_dets, img.kp.smem_nodes, img.kp.smem_tris, img.kp.smem_next,
+                                                     coop ? b / 32 : 0);
+                        Context* c = nullptr;
+                        st = create_from_image(img, &c);
+                        if (st) {  // this shape cannot be resident (shared memory, registers): skip it
+                            last_err = g_last_error;
+                            continue;
+                        }
+                        xmc_ledger led;
+                        st = run(c, 1, 0, std::max<uint64_t>(n / 4, 1), nullptr, &led);
+                        if (!st || st == XMC_ERR_BUDGET) st = run(c, 2, 0, n, nullptr, &led);
+                        free_context(c);
+                        if (st && st != XMC_ERR_BUDGET) return st;
+                        if (led.kernel_ms < best_t) {
+                            best_t = led.kernel_ms;
+                            best_o = img.opt;
+                        }
+                    }
                 }
-                xmc_ledger led;
-                st = run(c, 1, 0, std::max<uint64_t>(n / 4, 1), nullptr, &led);
-                if (!st || st == XMC_ERR_BUDGET) st = run(c, 2, 0, n, nullptr, &led);
-                free_context(c);
-                if (st && st != XMC_ERR_BUDGET) return st;
-                if (led.kernel_ms < best_t) {
-                    best_t = led.kernel_ms;
-                    best_o = img.opt;
-                }
-              }
             }
         }
     }

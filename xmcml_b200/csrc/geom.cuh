@@ -122,9 +122,10 @@ __host__ __device__ __forceinline__ Hit bvh_nearest(const float4* __restrict__ g
                     a = XMC_LDG(&g_tris[3 * i]); b = XMC_LDG(&g_tris[3 * i + 1]); c = XMC_LDG(&g_tris[3 * i + 2]);
                 }
                 const float t = tri_distance(a, b, c, ox, oy, oz, dx, dy, dz, retests);
-                // nearest wins; on equal distances the first triangle found keeps the hit; a
-                // distance equal to tmax still counts (the reference accepts distance <= step)
-                if (t >= tmin && t < INFINITY && (t < h.t || (t == h.t && h.tri < 0))) {
+                // nearest wins; equal distances keep the lower triangle index (as the grid search
+                // does, so both find the same hit); a distance equal to tmax still counts (the
+                // reference accepts distance <= step)
+                if (t >= tmin && t < INFINITY && (t < h.t || (t == h.t && (h.tri < 0 || i < h.tri)))) {
                     h.t = t;
                     h.tri = i;
                 }

@@ -277,7 +277,7 @@ bool gpu_lbvh_topology(const std::vector<float>& cen, int n, int device, std::ve
 int occupied_z_slabs(const GeomImage& g, float* lo, float* hi);
 
 // bvh.cpp: build the xy cell grid over the triangles of `g` (empty grid when there are none)
-void build_xy_grid(const GeomImage& g, GridImage* out);
+void build_xy_grid(const GeomImage& g, GridImage* out, int tris_per_cell = 2);
 
 // transport.cu: enqueue one transport kernel launch on ctx->stream (tallies must be zeroed).
 cudaError_t enqueue_transport(Context* ctx);

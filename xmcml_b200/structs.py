@@ -126,7 +126,7 @@ class XmcOptions(C.Structure):
                 ("beam_radius", C.c_double), ("max_steps_per_photon", C.c_uint64), ("device", C.c_int32),
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("photons_per_chunk", C.c_int32),
                 ("smem_nodes", C.c_int32), ("trajectory_log", C.c_int32), ("query_batch", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("grid_cell_tris", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 _LEDGER_COUNTS = ["photons_launched", "photons_terminated", "steps", "n_escaped_top", "n_escaped_bottom",

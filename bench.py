@@ -67,7 +67,9 @@ def parse_args():
                    help="workloads measured beside the headline one (comma list, '' for none)")
     p.add_argument("--extra-steps", type=int, default=3)
     p.add_argument("--no-roulette-variant", action="store_true")
-    p.add_argument("--no-autotune", action="store_true", help="default launch shape (profiling runs)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="fixed launch shape instead of the autotuner's (profiling runs): block 512, 32 photon ids "
+                        "per claim, cooperative queries in rounds of 8, 8 triangles per grid cell")
     return p.parse_args()
 
 
@@ -564,7 +566,7 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
     maps = not roulette
     kw = dict(roulette=roulette, scattering=maps, trajectories=maps, device=local)
     if args.no_autotune:
-        tuned, tune_ms = api.options(**kw), None
+        tuned, tune_ms = api.options(block_size=512, photons_per_chunk=32, query_batch=8, grid_cell_tris=8, **kw), None
     else:  # the project's launch-shape autotuner
         tuned, tune_ms = api.autotune(m, sample_photons=min(N, 1_000_000), **kw)
     t = api.Transport(m, tuned)

@@ -222,7 +222,7 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch):
+def run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch, tuned=None):
     """e2e photons/s through xmc_launch_omp with host InputInfo/OutputInfo (see module docstring).
 
     value: repeated LaunchOMP calls on one model (the library keeps the device image while the
@@ -259,7 +259,8 @@ def run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch):
     T = m.info.timeScaleSize
     out.close()
     # where a warm call's time goes: the same run through a context with LaunchOMP's options
-    t = api.Transport(m, roulette=False, scattering=True, trajectories=True, device=local)
+    t = api.Transport(m, tuned) if tuned is not None else api.Transport(m, roulette=False, scattering=True,
+                                                                        trajectories=True, device=local)
     out2 = api.Output(m)
     t.run(N, seed=777 + rank, output=out2)  # first run of a fresh context (staging allocation)
     t0 = time.perf_counter()
@@ -609,7 +610,11 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
 
     e2e = None
     if e2e_steps > 0:
-        e2e = run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch)
+        api.launch_set_options(tuned)  # the LaunchOMP replacement runs with the tuned shape as well
+        try:
+            e2e = run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch, tuned)
+        finally:
+            api.launch_set_options(None)
 
     cpu = None
     if rank == 0 and world == 1 and cpu_seconds > 0 and not args.no_cpu_baseline:

@@ -230,17 +230,17 @@ typedef struct xmc_options {
     double   beam_radius;          /* uniform-disk beam radius in mm around startPosition (0 = pencil) */
     uint64_t max_steps_per_photon; /* step budget per photon (0 = 10,000,000)                    */
     int32_t  device;               /* CUDA device ordinal (default 0)                            */
-    int32_t  block_size;           /* threads per block (0 = autotuned / default 256)             */
+    int32_t  block_size;           /* threads per block (0 = 512)                                  */
     int32_t  blocks_per_sm;        /* resident blocks per SM (0 = occupancy maximum)              */
-    int32_t  photons_per_chunk;    /* photon ids a warp claims at a time (0 = 64)                 */
+    int32_t  photons_per_chunk;    /* photon ids a warp claims at a time (0 = 32)                 */
     int32_t  smem_nodes;           /* BVH nodes staged in shared memory (-1 = none, 0 = auto)      */
     int32_t  trajectory_log;       /* XMC_DETECTOR_TRAJ: z-plane crossings logged per resident thread
                                     * (0 = 4096, at most 65536; -1 = no log, every detected photon
                                     * is replayed)                                                 */
     int32_t  query_batch;          /* cooperative ray queries: rays a warp collects (the lanes that
-                                    * need one wait) before it runs a query round; 0 or 1 = every
-                                    * iteration. A scheduling choice: tallies are the same bit for bit */
-    int32_t  grid_cell_tris;       /* triangles per cell the xy grid of short ray queries aims at (0 = 2;
+                                    * need one wait) before it runs a query round (0 = 8; 1 = every
+                                    * iteration). A scheduling choice: tallies are the same bit for bit */
+    int32_t  grid_cell_tris;       /* triangles per cell the xy grid of short ray queries aims at (0 = 8;
                                     * larger: coarser cells, fewer queries fall back to the BVH). A
                                     * speed choice: tallies are the same bit for bit              */
     int32_t  reserved[4];
@@ -376,6 +376,12 @@ int xmc_run_noalloc(const InputInfo* input, const xmc_options* opt, uint64_t see
  * 8 blocks of 256 threads per SM. Allocates and frees its own array on `device`. */
 int xmc_atomic_throughput(int device, unsigned log2_slots, unsigned adds_per_thread, double* atomics_per_s,
                           double* ms);
+
+/* No counterpart in the reference (LaunchOMP has no options argument). Sets the options
+ * xmc_launch_omp uses for its later calls in this process, e.g. the launch shape xmc_autotune found
+ * for the model (NULL: back to the defaults). xmc_launch_omp still sets XMC_SCATTERING_MAP and
+ * XMC_DETECTOR_TRAJ and takes the device from the calling thread; the options are copied. */
+int xmc_launch_set_options(const xmc_options* opt);
 
 /* Replaces LaunchOMP(InputInfo*, OutputInfo*, MCG59*, int)
  * (base/xmcml/xmcmlLauncher/launcher_omp.h:10, launcher_omp.cpp:123-163): runs

@@ -42,7 +42,7 @@ def test_version_and_defaults():
     o = S.XmcOptions()
     lib.xmc_default_options(C.byref(o))
     assert o.struct_size == C.sizeof(S.XmcOptions)
-    assert o.roulette_chance == 0.1 and o.max_steps_per_photon == 10_000_000 and o.photons_per_chunk == 64
+    assert o.roulette_chance == 0.1 and o.max_steps_per_photon == 10_000_000 and o.photons_per_chunk == 32
 
 
 def _ctypes_offsets():

@@ -608,3 +608,35 @@ def test_autotune_picks_a_shape_with_identical_tallies(tmp_path):
         assert np.array_equal(res[0][0][k], res[1][0][k]), k
     for k in S.LEDGER_TERMS:
         assert res[0][1][k + "_fx"] == res[1][1][k + "_fx"]
+
+
+def test_launch_omp_uses_the_options_set_for_it(tmp_path):
+    """xmc_launch_set_options: the LaunchOMP replacement runs with a caller's launch shape (as
+    xmc_autotune returns it) and gives the same OutputInfo as with the defaults, bit for bit; NULL
+    restores the defaults."""
+    n = 20_000
+    xml, surf = scenes.height_field_tissue(photons=n, grid=64, time_bins=10).write(str(tmp_path), "setopt")
+    m = api.Model(xml, surf)
+
+    def via_launch():
+        out = api.Output(m)
+        g = S.MCG59()
+        g.value, g.offset = 4242, 1
+        api.launch_omp(m, out, g, 0)
+        G = out.info.gridSize
+        traj = np.stack([np.ctypeslib.as_array(out.info.detectorInfo[d].trajectory, shape=(G,)).copy()
+                         for d in range(out.info.numberOfDetectors)])
+        return out.detector_weights(), out.absorption.copy(), traj
+
+    try:
+        a = via_launch()
+        api.launch_set_options(api.options(lane_queries=True, grid_cell_tris=32, block_size=256, photons_per_chunk=64))
+        b = via_launch()
+        api.launch_set_options(api.options(query_batch=16, grid_cell_tris=2))
+        c = via_launch()
+    finally:
+        api.launch_set_options(None)
+    for other in (b, c):
+        for x, y in zip(a, other):
+            assert np.array_equal(x, y)
+    _lib.check(_lib.load().xmc_launch_release())

@@ -45,6 +45,7 @@ def load(path: str | None = None) -> C.CDLL:
         "xmc_launch": (C.c_int, [P(S.InputInfo), P(S.OutputInfo), C.c_uint64, C.c_uint64, P(S.XmcOptions),
                                  P(S.XmcLedger)]),
         "xmc_launch_omp": (C.c_int, [P(S.InputInfo), P(S.OutputInfo), P(S.MCG59), C.c_int]),
+        "xmc_launch_set_options": (C.c_int, [P(S.XmcOptions)]),
         "xmc_init_output": (None, [P(S.InputInfo), P(S.OutputInfo)]),
         "xmc_free_output": (None, [P(S.OutputInfo)]),
         "xmc_parse_input_file": (C.c_bool, [C.c_char_p, P(S.InputInfo)]),
@@ -119,5 +120,5 @@ EXPORTS = [
     "xmc_mlp_create", "xmc_mlp_param_count", "xmc_mlp_set_params", "xmc_mlp_get_params", "xmc_mlp_forward",
     "xmc_mlp_forward_timed", "xmc_mlp_gradients", "xmc_mlp_set_dataset", "xmc_mlp_train", "xmc_mlp_destroy",
     "xmc_mlp_set_output_weights", "xmc_weight_integral_table", "xmc_launch_release",
-    "xmc_gemm_bf16", "xmc_atomic_throughput", "xmc_autotune",
+    "xmc_gemm_bf16", "xmc_atomic_throughput", "xmc_autotune", "xmc_launch_set_options",
 ]

@@ -200,6 +200,11 @@ def autotune(model: Model, sample_photons: int = 1_000_000, **kw) -> tuple:
     return best, ms.value
 
 
+def launch_set_options(opts: Optional[S.XmcOptions]) -> None:
+    """Options xmc_launch_omp uses from now on (e.g. autotune's result); None restores the defaults."""
+    check(load().xmc_launch_set_options(C.byref(opts) if opts is not None else None))
+
+
 def launch_omp(model: Model, output: Output, rng: S.MCG59, num_threads: int = 0) -> int:
     """LaunchOMP(InputInfo*, OutputInfo*, MCG59*, int) on the GPU (launcher_omp.cpp:123-163)."""
     st = load().xmc_launch_omp(C.byref(model.info), C.byref(output.info), C.byref(rng), num_threads)

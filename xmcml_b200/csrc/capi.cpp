@@ -167,7 +167,7 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
         opt.struct_size = sizeof(xmc_options);
         if (opt.roulette_chance == 0) opt.roulette_chance = 0.1;
         if (opt.max_steps_per_photon == 0) opt.max_steps_per_photon = 10000000ull;
-        if (opt.photons_per_chunk <= 0) opt.photons_per_chunk = 64;
+        if (opt.photons_per_chunk <= 0) opt.photons_per_chunk = 32;
     }
     int st = validate(in, opt);
     if (st) return st;
@@ -314,7 +314,7 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.n_nodes = geom.n_nodes;
     kp.n_tris = geom.n_tris;
     kp.n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
-    build_xy_grid(geom, &img->grid, opt.grid_cell_tris > 0 ? opt.grid_cell_tris : 2);
+    build_xy_grid(geom, &img->grid, opt.grid_cell_tris > 0 ? opt.grid_cell_tris : 8);
     kp.grid_x0 = img->grid.x0;
     kp.grid_y0 = img->grid.y0;
     kp.grid_icx = img->grid.icx;
@@ -323,8 +323,8 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.grid_ny = img->grid.ny;
     kp.n_big = (int)(img->grid.big.size() / 4);
     kp.coop_query = (opt.flags & XMC_LANE_QUERIES) ? 0 : 1;
-    kp.query_batch = std::max(1, std::min(32, (int)opt.query_batch));
-    const int block = opt.block_size > 0 ? opt.block_size : 256;
+    kp.query_batch = opt.query_batch > 0 ? std::min(32, (int)opt.query_batch) : 8;
+    const int block = opt.block_size > 0 ? opt.block_size : 512;
     img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next, kp.coop_query ? block / 32 : 0);
     // ---- biasing (mcml_kernel.cpp:325-440) ----
     kp.use_bias = in->useBiasing ? 1 : 0;
@@ -568,7 +568,7 @@ static int create_from_image(const HostImage& img, Context** out) {
     kp.replay_count = (unsigned long long*)c->d_replay_count;
 
     // ---- launch shape ----
-    c->block = opt.block_size > 0 ? opt.block_size : 256;
+    c->block = opt.block_size > 0 ? opt.block_size : 512;
     if (c->block % 32 != 0 || c->block > 1024) return bail(fail(XMC_ERR_INVALID_INPUT, "block_size must be a multiple of 32 <= 1024"));
     int occ = 0;
     CK(transport_occupancy(c->block, c->smem_bytes, &occ, c->kp.use_bias != 0));
@@ -773,7 +773,7 @@ void xmc_default_options(xmc_options* o) {
     o->struct_size = sizeof(xmc_options);
     o->roulette_chance = 0.1;
     o->max_steps_per_photon = 10000000ull;
-    o->photons_per_chunk = 64;
+    o->photons_per_chunk = 32;
 }
 
 int xmc_create(const InputInfo* input, const xmc_options* opt, xmc_context** out_ctx) {
@@ -995,6 +995,11 @@ uint64_t input_fingerprint(const InputInfo* in, const xmc_options* opt) {
     return f.h;
 }
 
+// Options xmc_launch_omp uses (xmc_launch_set_options; defaults until set).
+std::mutex g_omp_opts_mutex;
+xmc_options g_omp_opts{};
+bool g_omp_opts_set = false;
+
 // The device context of the last model run through xmc_launch, kept for the next call on the same
 // model contents (the reference's launchers call LaunchOMP repeatedly on one InputInfo).
 std::mutex g_launch_mutex;
@@ -1037,6 +1042,15 @@ int xmc_launch_release(void) {
     return XMC_OK;
 }
 
+int xmc_launch_set_options(const xmc_options* opt) {
+    std::lock_guard<std::mutex> lock(g_omp_opts_mutex);
+    g_omp_opts_set = opt && opt->struct_size;
+    xmc_default_options(&g_omp_opts);
+    if (g_omp_opts_set) std::memcpy(&g_omp_opts, opt, std::min((size_t)opt->struct_size, sizeof(g_omp_opts)));
+    g_omp_opts.struct_size = sizeof(g_omp_opts);
+    return XMC_OK;
+}
+
 int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* rng, int numThreads) {
     (void)numThreads;
     if (!input || !output || !rng) {
@@ -1045,8 +1059,12 @@ int xmc_launch_omp(InputInfo* input, OutputInfo* output, MCG59* rng, int numThre
         return XMC_ERR_INVALID_INPUT;
     }
     xmc_options opt;
-    xmc_default_options(&opt);
-    opt.flags = XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ;  // every tally LaunchOMP fills
+    {
+        std::lock_guard<std::mutex> lock(g_omp_opts_mutex);
+        if (g_omp_opts_set) opt = g_omp_opts;
+        else xmc_default_options(&opt);
+    }
+    opt.flags |= XMC_SCATTERING_MAP | XMC_DETECTOR_TRAJ;  // every tally LaunchOMP fills
     int dev = 0;  // LaunchOMP has no device argument: the caller's current device
     if (cudaGetDevice(&dev) == cudaSuccess) opt.device = dev;
     int st = xmc_launch(input, output, rng[0].value, 0, &opt, nullptr);

@@ -19,6 +19,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -418,6 +419,8 @@ struct xmc_mlp {
     std::map<int, cudaGraphExec_t> fwd_graphs;
     float g_lr = 0, g_b1 = 0, g_b2 = 0, g_eps = 0;
     uint64_t g_seed = 0;
+    float* h_y = nullptr;           // pinned staging of the outputs read back by xmc_mlp_forward (lazy)
+    size_t h_y_floats = 0;
 };
 
 namespace xmc {
@@ -440,6 +443,7 @@ void free_mlp(xmc_mlp* m) {
         if (p) cudaFree(p);
     for (cudaEvent_t e : m->ev)
         if (e) cudaEventDestroy(e);
+    if (m->h_y) cudaFreeHost(m->h_y);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
 }
@@ -755,8 +759,33 @@ extern "C" int xmc_mlp_forward(xmc_mlp* m, const float* x, int rows, float* y, d
     st = enqueue_forward(m, rows, false);
     if (st) return st;
     XM_CUDA(cudaEventRecord(m->ev[1], m->stream));
-    XM_CUDA(cudaMemcpyAsync(y, m->y, sizeof(float) * (size_t)rows * m->spec.n_out, cudaMemcpyDeviceToHost, m->stream));
+    // outputs through pinned staging (kept by the model, sized for its row capacity), then into the
+    // caller's array on up to 8 host threads
+    const size_t nf = (size_t)rows * m->spec.n_out;
+    if (m->h_y_floats < nf) {
+        if (m->h_y) cudaFreeHost(m->h_y);
+        m->h_y = nullptr;
+        m->h_y_floats = 0;
+        XM_CUDA(cudaHostAlloc((void**)&m->h_y, sizeof(float) * (size_t)m->cap * m->spec.n_out, cudaHostAllocDefault));
+        m->h_y_floats = (size_t)m->cap * m->spec.n_out;
+    }
+    XM_CUDA(cudaMemcpyAsync(m->h_y, m->y, sizeof(float) * nf, cudaMemcpyDeviceToHost, m->stream));
     XM_CUDA(cudaStreamSynchronize(m->stream));
+    const unsigned parts = nf < ((size_t)1 << 20) ? 1u : std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t per = (nf + parts - 1) / parts;
+    auto copy_part = [&](unsigned p) {
+        const size_t a = std::min(nf, p * per), b = std::min(nf, a + per);
+        if (a < b) std::memcpy(y + a, m->h_y + a, sizeof(float) * (b - a));
+    };
+    std::vector<std::thread> pool;
+    unsigned started = 1;
+    try {
+        for (; started < parts; ++started) pool.emplace_back(copy_part, started);
+    } catch (...) {
+    }
+    copy_part(0);
+    for (unsigned p = started; p < parts; ++p) copy_part(p);
+    for (auto& th : pool) th.join();
     float t = 0.0f;
     XM_CUDA(cudaEventElapsedTime(&t, m->ev[0], m->ev[1]));
     if (ms) *ms = t;

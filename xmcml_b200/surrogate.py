@@ -86,11 +86,13 @@ class MLP:
             rp = pad_rows(r)
             if rp != r:
                 xb = np.concatenate([xb, np.zeros((rp - r, self.n_in), np.float32)])
-            y = np.zeros((rp, self.n_out), dtype=np.float32)
+            y = np.empty((rp, self.n_out), dtype=np.float32)
             t = C.c_double(0.0)
             check(self._lib.xmc_mlp_forward(self._m, xb.ctypes.data_as(FP), rp, y.ctypes.data_as(FP), C.byref(t)))
             outs.append(y[:r])
             ms += t.value
+        if len(outs) == 1:
+            return outs[0], ms
         return np.concatenate(outs) if outs else np.zeros((0, self.n_out), np.float32), ms
 
     def forward_timed(self, rows: int, reps: int = 20) -> float:

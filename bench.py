@@ -569,7 +569,7 @@ def measure_transport(args, workload, N, steps, warmup, e2e_steps, rank, world, 
     if args.no_autotune:
         tuned, tune_ms = api.options(block_size=512, photons_per_chunk=32, query_batch=8, grid_cell_tris=8, **kw), None
     else:  # the project's launch-shape autotuner
-        tuned, tune_ms = api.autotune(m, sample_photons=min(N, 1_000_000), **kw)
+        tuned, tune_ms = api.autotune(m, sample_photons=min(N, 2_000_000), **kw)
     t = api.Transport(m, tuned)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
     for w in range(warmup):  # disjoint photon ids per rank and step

@@ -330,8 +330,9 @@ int xmc_destroy(xmc_context* ctx);
  * times `sample_photons` photons (0 = 1e6) under every candidate: xy-grid density grid_cell_tris
  * {2, 8, 32} triangles per cell, block size {256, 512} at the occupancy maximum, photon ids a warp
  * claims from the dispenser at a time {32, 64}, and the ray-query scheme (warp-cooperative with
- * query_batch {1, 8, 16}, or lane by lane with XMC_LANE_QUERIES): 48 candidates. *best gets `base`
- * with the fastest one, *best_ms (may be NULL) its kernel time. Every candidate gives bit-identical
+ * query_batch {1, 8, 16}, or lane by lane with XMC_LANE_QUERIES): 48 candidates, each timed once, the
+ * four fastest twice more on other photons. *best gets `base` with the fastest one, *best_ms (may be
+ * NULL) its best kernel time. Every candidate gives bit-identical
  * tallies: a photon's random numbers, its candidate triangles' arithmetic and the choice among equal
  * distances (the lower triangle index) do not depend on them. */
 int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sample_photons, xmc_options* best,

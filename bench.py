@@ -267,11 +267,13 @@ def run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch, tuned=Non
     led = t.run(N, seed=777 + rank, output=out2)
     wall_ms = (time.perf_counter() - t0) * 1e3
     image_b = led["h2d_bytes"]
+    # read back per call, as the library counts it: absorption and scattering maps (u64), detector and
+    # time-bin tallies, the run and replay ledgers, status, and the trajectory maps as their non-zero
+    # cells (u32 cell + u64 count each, after the per-block offsets)
+    d2h = led["d2h_bytes"]
+    dense_d2h = 8 * grid * (2 + D) + 32 * D + 32 * D * T + 2 * 8 * 32 + 16
     t.close()
     out2.close()
-    # read back per call: absorption, scattering and D trajectory maps (u64), detector and time-bin
-    # tallies (4 u64 each), the run and replay ledgers, status
-    d2h = 8 * grid * (2 + D) + 32 * D + 32 * D * T + 2 * 8 * 32 + 16
     m.info.bvhTree = None
     lib.xmc_free_bvh_tree(tree)
     return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(d2h),
@@ -280,6 +282,7 @@ def run_e2e(m, N, e2e_steps, rank, local, world, barrier, dist, torch, tuned=Non
                         "a warm call copies no input buffer (seed and counts travel as kernel arguments)",
             "cold": {"value": world * N / cold_s, "unit": UNIT, "h2d_bytes": int(image_b), "d2h_bytes": int(d2h),
                      "seconds": cold_s},
+            "d2h_dense_bytes": int(dense_d2h),
             "breakdown_ms": {"kernels": led["kernel_ms"], "device_total": led["total_ms"], "host_wall": wall_ms,
                              "trajectory_replayed": led["n_trajectory_replayed"]}}
 

@@ -520,10 +520,11 @@ def test_launch_keeps_context_only_for_unchanged_models(tmp_path):
 
 @pytest.mark.parametrize("partitions", [(100, 100, 100), (40, 40, 40)])
 def test_output_maps_accumulate_the_device_maps_exactly(tmp_path, partitions):
-    """xmc_run with an OutputInfo adds the run's maps into the caller's arrays (copied map by map and
-    added by host threads while later maps copy; 1e6 cells use several threads, 64,000 one): after
-    two runs every detector's trajectory map is exactly the sum of the two runs' integer maps, and the
-    scattering map their FP64 value."""
+    """xmc_run with an OutputInfo adds the run's maps into the caller's arrays (the trajectory maps read
+    back as the list of their non-zero cells, added by host threads; 1e6 cells use several threads,
+    64,000 one): after two runs every detector's trajectory map is exactly the sum of the two runs'
+    integer maps, and the scattering map their FP64 value. The ledger's read-back bytes count 12 bytes
+    per non-zero trajectory cell over a part that does not depend on the run."""
     n = 30_000
     sc = scenes.height_field_tissue(photons=n, grid=64, time_bins=10, area_partitions=partitions)
     xml, surf = sc.write(str(tmp_path), "acc")
@@ -533,12 +534,17 @@ def test_output_maps_accumulate_the_device_maps_exactly(tmp_path, partitions):
     G, D = out.info.gridSize, m.n_detectors
     traj_sum = np.zeros((D, G), dtype=np.uint64)
     scat_sum = np.zeros(G, dtype=np.float64)
+    fixed = set()
     for seed in (3, 4):
-        t.run(n, seed=seed, output=out)
+        led = t.run(n, seed=seed, output=out)
         maps = t.maps()
         traj_sum += maps["trajectory"][:D]
         scat_sum += maps["scattering"].astype(np.float64) / WEIGHT_SCALE
+        nz = int(np.count_nonzero(maps["trajectory"][:D]))
+        assert 0 < nz < D * G
+        fixed.add(int(led["d2h_bytes"]) - 12 * nz)
     t.close()
+    assert len(fixed) == 1 and fixed.pop() > 8 * G
     got = np.stack([np.ctypeslib.as_array(out.info.detectorInfo[d].trajectory, shape=(G,)) for d in range(D)])
     assert traj_sum.sum() > 0
     assert np.array_equal(got, traj_sum)

@@ -18,8 +18,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libxmcml_b200.so")
 
-SOURCES = ["transport.cu", "batch.cu", "surrogate.cu", "weight_table.cu", "noalloc.cu", "bvh_gpu.cu", "capi.cpp", "io.cpp",
-           "bvh.cpp"]
+SOURCES = ["transport.cu", "batch.cu", "surrogate.cu", "weight_table.cu", "noalloc.cu", "bvh_gpu.cu", "sparse_maps.cu",
+           "capi.cpp", "io.cpp", "bvh.cpp"]
 HEADERS = ["xmc_internal.h", "geom.cuh", "photon.cuh", "tc_gemm.cuh", "mlp_fused.cuh"]
 
 NVCC_FLAGS = [

@@ -40,10 +40,12 @@ static void free_context(Context* c) {
     void* dbufs[] = {c->d_nodes, c->d_tris, c->d_next, c->d_dets, c->d_absorb, c->d_det,
                      c->d_tbin, c->d_ledger, c->d_counter, c->d_status, c->d_scatter, c->d_traj,
                      c->d_replay, c->d_replay_count, c->d_replay_ledger, c->d_cells, c->d_cell_z, c->d_cell_entries,
-                     c->d_big, c->d_cancel, c->d_wtab, c->d_xlog, c->d_cell_runs};
+                     c->d_big, c->d_cancel, c->d_wtab, c->d_xlog, c->d_cell_runs, c->d_nz_counts, c->d_nz_offsets,
+                     c->d_nz_tmp, c->d_nz_idx, c->d_nz_val};
     for (void* p : dbufs)
         if (p) cudaFree(p);
-    void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status, c->h_maps};
+    void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status, c->h_maps,
+                     c->h_nz_offsets, c->h_nz_idx, c->h_nz_val};
     for (void* p : hbufs)
         if (p) cudaFreeHost(p);
     for (cudaEvent_t& e : c->ev)
@@ -610,8 +612,8 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     }
     const bool want_scat = out && scat && out->scattering;
     const bool want_traj = out && traj && c->n_dets > 0;
-    if (want_scat || want_traj) {  // pinned staging of the maps, kept by the context
-        const size_t need = absorb_b * ((want_scat ? 1 : 0) + (want_traj ? (size_t)c->n_dets : 0));
+    if (want_scat) {  // pinned staging of the scattering map, kept by the context
+        const size_t need = absorb_b;
         if (c->h_maps_bytes < need) {
             if (c->h_maps) cudaFreeHost(c->h_maps);
             c->h_maps = nullptr;
@@ -688,14 +690,64 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
     if (traj)
         XMC_CUDA(cudaMemcpyAsync(c->h_ledger + kLedgerSlots, c->d_replay_ledger, led_b, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
-    // maps: one pinned staging buffer (allocated before the run) for the scattering map and every
-    // detector's trajectory map
+    // maps: the scattering map through its pinned staging; the trajectory maps as the list of their
+    // non-zero cells (count pass and scan, the list's length to the host, write pass, copy)
     unsigned long long* hs = c->h_maps;
-    unsigned long long* ht = c->h_maps + (want_scat ? (size_t)c->grid_size : 0);
     const size_t G = (size_t)c->grid_size;
     if (want_scat) XMC_CUDA(cudaMemcpyAsync(hs, c->d_scatter, absorb_b, cudaMemcpyDeviceToHost, c->stream));
-    if (want_traj)
-        XMC_CUDA(cudaMemcpyAsync(ht, c->d_traj, absorb_b * (size_t)c->n_dets, cudaMemcpyDeviceToHost, c->stream));
+    size_t nz_total = 0;
+    std::vector<size_t> map_start;
+    if (want_traj) {
+        const size_t D = (size_t)c->n_dets;
+        const size_t nb = (size_t)sparse_blocks_per_map(G) * D;
+        if (!c->d_nz_counts) {
+            XMC_CUDA(cudaMalloc(&c->d_nz_counts, sizeof(unsigned long long) * nb));
+            XMC_CUDA(cudaMalloc(&c->d_nz_offsets, sizeof(unsigned long long) * nb));
+            XMC_CUDA(cudaHostAlloc((void**)&c->h_nz_offsets, sizeof(unsigned long long) * (nb + 1), cudaHostAllocDefault));
+        }
+        XMC_CUDA(sparse_maps_count((const unsigned long long*)c->d_traj, G, (int)D, c->d_nz_counts,
+                                   c->d_nz_offsets, &c->d_nz_tmp, &c->nz_tmp_bytes, c->stream));
+        XMC_CUDA(cudaMemcpyAsync(c->h_nz_offsets, c->d_nz_offsets, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost,
+                                 c->stream));
+        XMC_CUDA(cudaMemcpyAsync(c->h_nz_offsets + nb, c->d_nz_counts + nb - 1, sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, c->stream));
+        XMC_CUDA(cudaStreamSynchronize(c->stream));
+        nz_total = (size_t)(c->h_nz_offsets[nb - 1] + c->h_nz_offsets[nb]);
+        const size_t bpm = nb / D;
+        map_start.resize(D + 1);
+        for (size_t d = 0; d < D; ++d) map_start[d] = (size_t)c->h_nz_offsets[d * bpm];
+        map_start[D] = nz_total;
+        if (nz_total > c->nz_cap) {
+            const size_t cap = nz_total + nz_total / 4 + 1024;
+            if (c->d_nz_idx) cudaFree(c->d_nz_idx);
+            if (c->d_nz_val) cudaFree(c->d_nz_val);
+            c->d_nz_idx = nullptr;
+            c->d_nz_val = nullptr;
+            c->nz_cap = 0;
+            XMC_CUDA(cudaMalloc(&c->d_nz_idx, sizeof(unsigned) * cap));
+            XMC_CUDA(cudaMalloc(&c->d_nz_val, sizeof(unsigned long long) * cap));
+            c->nz_cap = cap;
+        }
+        if (nz_total > c->h_nz_cap) {
+            const size_t cap = c->nz_cap;
+            if (c->h_nz_idx) cudaFreeHost(c->h_nz_idx);
+            if (c->h_nz_val) cudaFreeHost(c->h_nz_val);
+            c->h_nz_idx = nullptr;
+            c->h_nz_val = nullptr;
+            c->h_nz_cap = 0;
+            XMC_CUDA(cudaHostAlloc((void**)&c->h_nz_idx, sizeof(unsigned) * cap, cudaHostAllocDefault));
+            XMC_CUDA(cudaHostAlloc((void**)&c->h_nz_val, sizeof(unsigned long long) * cap, cudaHostAllocDefault));
+            c->h_nz_cap = cap;
+        }
+        XMC_CUDA(sparse_maps_write((const unsigned long long*)c->d_traj, G, (int)D, c->d_nz_offsets, c->d_nz_idx,
+                                   c->d_nz_val, c->stream));
+        if (nz_total) {
+            XMC_CUDA(cudaMemcpyAsync(c->h_nz_idx, c->d_nz_idx, sizeof(unsigned) * nz_total, cudaMemcpyDeviceToHost,
+                                     c->stream));
+            XMC_CUDA(cudaMemcpyAsync(c->h_nz_val, c->d_nz_val, sizeof(unsigned long long) * nz_total,
+                                     cudaMemcpyDeviceToHost, c->stream));
+        }
+    }
     XMC_CUDA(cudaStreamSynchronize(c->stream));
     float k_ms = 0, t_ms = 0;
     XMC_CUDA(cudaEventElapsedTime(&k_ms, c->ev[1], c->ev[2]));
@@ -724,9 +776,9 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
             }
         }
         // voxel arrays on up to 16 host threads, each owning a slice of the grid: absorption and
-        // scattering (FP64 from fixed point) and every detector's trajectory map, where only the
-        // cells a photon crossed (non-zero counts) touch the caller's arrays
-        const unsigned hw = host_threads_for(G * (1 + (want_traj ? (size_t)c->n_dets : 0)));
+        // scattering (FP64 from fixed point); then the trajectory maps' non-zero cells, each thread a
+        // slice of the list (a cell appears once per map, so the slices touch disjoint cells)
+        const unsigned hw = host_threads_for(G);
         const size_t per = (G + hw - 1) / hw;
         parallel_parts(hw, [&](unsigned t) {
             const size_t a = std::min(G, t * per), b = std::min(G, a + per);
@@ -734,21 +786,34 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
                 for (size_t i = a; i < b; ++i) out->absorption[i] += (double)c->h_absorb[i] * inv_scale;
             if (want_scat)
                 for (size_t i = a; i < b; ++i) out->scattering[i] += (double)hs[i] * inv_scale;
-            for (int d = 0; want_traj && d < c->n_dets; ++d) {
-                DetectorInfo& D = out->detectorInfo[d];
-                if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
-                const unsigned long long* src = ht + d * G;
-                for (size_t i = a; i < b; ++i)
-                    if (src[i]) D.trajectory[i] += src[i];
-            }
         });
+        if (want_traj && nz_total) {
+            const unsigned hz = host_threads_for(nz_total);
+            const size_t pz = (nz_total + hz - 1) / hz;
+            parallel_parts(hz, [&](unsigned t) {
+                const size_t a = std::min(nz_total, t * pz), b = std::min(nz_total, a + pz);
+                if (a >= b) return;
+                size_t d = (size_t)(std::upper_bound(map_start.begin(), map_start.end(), a) - map_start.begin()) - 1;
+                for (size_t e = a; e < b; ++e) {
+                    while (e >= map_start[d + 1]) ++d;
+                    DetectorInfo& D = out->detectorInfo[d];
+                    if (D.trajectory && D.trajectorySize == c->grid_size) D.trajectory[c->h_nz_idx[e]] += c->h_nz_val[e];
+                }
+            });
+        }
     }
     if (led) {
         fill_ledger(L, c->w0_fx, n, led);
         led->kernel_ms = k_ms;
         led->total_ms = t_ms;
         led->h2d_bytes = c->h2d_bytes + sizeof(KParams);
-        led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16;
+        // every device-to-host copy of this call: tallies, ledgers and status, the scattering map, and
+        // the sparse trajectory maps (block offsets, then the (cell, count) pairs)
+        size_t maps_b = want_scat ? absorb_b : 0;
+        if (want_traj)
+            maps_b += sizeof(unsigned long long) * ((size_t)c->n_dets * sparse_blocks_per_map(G) + 1) +
+                      (sizeof(unsigned) + sizeof(unsigned long long)) * nz_total;
+        led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16 + (traj ? led_b : 0) + maps_b;
         led->n_replay_mismatch = traj ? c->h_ledger[kLedgerSlots + L_N_REPLAY_MISMATCH] : 0;
         led->n_trajectory_replayed = traj ? c->last_replayed : 0;
     }

@@ -212,8 +212,15 @@ struct Context {
     unsigned long long* h_absorb = nullptr; unsigned long long* h_det = nullptr;
     unsigned long long* h_tbin = nullptr;
     unsigned long long* h_ledger = nullptr;  // [2 x kLedgerSlots]: the run pass, then the replay pass
-    unsigned long long* h_maps = nullptr;   // pinned staging of the scattering and trajectory maps (lazy)
+    unsigned long long* h_maps = nullptr;   // pinned staging of the scattering map (lazy)
     size_t h_maps_bytes = 0;
+    // sparse read-back of the trajectory maps (lazy): block counts and their scan, the non-zero cells as
+    // (cell, count) pairs grouped by map, and their pinned staging
+    unsigned long long* d_nz_counts = nullptr; unsigned long long* d_nz_offsets = nullptr;
+    void* d_nz_tmp = nullptr; size_t nz_tmp_bytes = 0;
+    unsigned* d_nz_idx = nullptr; unsigned long long* d_nz_val = nullptr; size_t nz_cap = 0;
+    unsigned long long* h_nz_offsets = nullptr;  // [maps x blocks per map + 1]: offsets, then the last count
+    unsigned* h_nz_idx = nullptr; unsigned long long* h_nz_val = nullptr; size_t h_nz_cap = 0;
     int* h_status = nullptr;
     uint64_t last_n = 0;
     double last_kernel_ms = 0.0, last_total_ms = 0.0;
@@ -281,6 +288,12 @@ void build_xy_grid(const GeomImage& g, GridImage* out, int tris_per_cell = 2);
 
 // transport.cu: enqueue one transport kernel launch on ctx->stream (tallies must be zeroed).
 cudaError_t enqueue_transport(Context* ctx);
+// sparse_maps.cu: blocks of cells per map, and the two passes of the sparse map read-back
+unsigned sparse_blocks_per_map(size_t cells);
+cudaError_t sparse_maps_count(const unsigned long long* maps, size_t cells, int n_maps, unsigned long long* counts,
+                              unsigned long long* offsets, void** scan_tmp, size_t* scan_tmp_bytes, cudaStream_t st);
+cudaError_t sparse_maps_write(const unsigned long long* maps, size_t cells, int n_maps, const unsigned long long* offsets,
+                              unsigned* idx, unsigned long long* val, cudaStream_t st);
 // transport.cu: occupancy of the kernel for a block size and dynamic shared memory.
 cudaError_t transport_occupancy(int block, size_t smem, int* blocks_per_sm, bool bias = false);
 // transport.cu: Philox blocks computed on the device (self test).

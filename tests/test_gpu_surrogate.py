@@ -228,13 +228,14 @@ def test_inverse_fit_with_network_and_monte_carlo_check():
 
 @pytest.mark.parametrize("n_in,hidden,n_hidden,n_out,rows", [(15, 256, 4, 1000, 65536), (15, 256, 4, 1000, 128),
                                                              (7, 128, 2, 300, 1280), (3, 256, 1, 4, 256),
-                                                             (5, 256, 3, 30, 512)])
+                                                             (5, 256, 3, 30, 512), (7, 128, 3, 520, 38528)])
 def test_fused_forward_matches_layered_and_oracle(n_in, hidden, n_hidden, n_out, rows):
     """The fused forward kernel (every layer of a 128-row tile on chip, weights streamed by TMA,
     outputs stored by TMA) against the per-layer GEMM path on the same parameters, and against the
     oracle. The two GPU paths round the same BF16 activations except where their SiLU evaluations
     (tanh form vs exponential form) straddle a rounding boundary. n_out = 30 is not a multiple of
-    4: the fused path does not apply and both calls run per layer."""
+    4: the fused path does not apply and both calls run per layer. 38,528 rows are 301 tiles, so some
+    CTAs run two tiles side by side and some a third one alone; n_out = 520 clips an output box."""
     rng = np.random.default_rng(rows + n_out)
     p = R.init_params(rng, n_in, hidden, n_hidden, n_out)
     p[-n_out:] = rng.normal(0, 0.1, n_out)

@@ -333,8 +333,8 @@ int make_map(CUtensorMap* map, const void* ptr, uint64_t rows, uint64_t cols, ui
     return XMC_OK;
 }
 
-// Tensor map of the FP32 output [rows x n_out] stored in 32 x 32 boxes with the 128-byte swizzle
-// (the fused forward's staging layout); columns past n_out are clipped by the store.
+// Tensor map of the FP32 output [rows x n_out] stored in boxes of 32 rows x 16 columns with the
+// 64-byte swizzle (the fused forward's staging layout); columns past n_out are clipped by the store.
 int make_out_map(CUtensorMap* map, float* y, uint64_t rows, uint64_t n_out) {
     int st = get_encoder();
     if (st) return st;
@@ -342,10 +342,10 @@ int make_out_map(CUtensorMap* map, float* y, uint64_t rows, uint64_t n_out) {
         return mfail(XMC_ERR_INVALID_INPUT, "tensor map: misaligned output");
     const cuuint64_t dims[2] = {n_out, rows};
     const cuuint64_t strides[1] = {n_out * 4};
-    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t box[2] = {(cuuint32_t)fused::kOutCols, 32};
     const cuuint32_t es[2] = {1, 1};
     CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, y, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                          CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return mfail(XMC_ERR_DEVICE, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
     return XMC_OK;
 }

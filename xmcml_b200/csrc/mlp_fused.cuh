@@ -14,14 +14,14 @@
 // layer's MMAs of one tile overlap the bias + SiLU epilogue of the other, and the output stores of one
 // overlap the MMAs of the other.
 //
-// Roles (320 threads): warp 8 lane 0 issues the TMA loads (the X tiles and the weights, 64 K-columns
-// per stage through a 2-stage ring); warp 9 lane 0 issues tcgen05.mma (M = 128, N = hidden or 256,
-// K = 16) into its slot's 256-column TMEM accumulator and commits to mbarriers; warps 0-7 drain an
-// accumulator with tcgen05.ld (warp w: TMEM lanes 32 (w % 4).., the column half w / 4). A hidden
+// Roles (576 threads): warp 16 lane 0 issues the TMA loads (the X tiles and the weights, 64 K-columns
+// per stage through a 2-stage ring); warp 17 lane 0 issues tcgen05.mma (M = 128, N = hidden or 256,
+// K = 16) into its slot's 256-column TMEM accumulator and commits to mbarriers; warps 0-15 drain an
+// accumulator with tcgen05.ld (warp w: TMEM lanes 32 (w % 4).., the column quarter w / 4). A hidden
 // layer's epilogue adds the bias, applies SiLU and writes the BF16 activations back into the slot's H
 // in the 128-byte-swizzled K-major layout the next layer's MMAs read (then fence.proxy.async and an
 // mbarrier arrive); the output epilogue adds the bias and stores 32-row x 16-column FP32 boxes
-// through two alternating 64-byte-swizzled staging buffers per warp with TMA
+// through a 64-byte-swizzled staging buffer per warp with TMA
 // (cp.async.bulk.tensor store). The X tile of a slot's next tile lands in H once the MMAs of the
 // slot's last output chunk have read it.
 //
@@ -36,7 +36,7 @@ namespace fused {
 
 constexpr int kMaxL = 9;
 constexpr int kSlots = 2;     // tiles in flight per CTA
-constexpr int kEpiWarps = 8;  // warp w reads TMEM lanes 32 (w % 4).. and column half w / 4
+constexpr int kEpiWarps = 16;  // warp w reads TMEM lanes 32 (w % 4).. and column quarter w / 4
 constexpr int kColGroups = kEpiWarps / 4;
 constexpr int kThreads = 32 * (kEpiWarps + 2);
 constexpr int kWStages = 2;                // weight ring depth (stages of 64 K-columns)
@@ -46,7 +46,7 @@ constexpr int kHBytes = 4 * kKBlockBytes;  // activations of one slot, hidden <=
 constexpr int kWBytes = 256 * 64 * 2;      // weight stage: up to 256 rows x 64 columns
 constexpr int kOutCols = 16;               // columns of one output box (64 bytes of FP32)
 constexpr int kOutBox = 32 * kOutCols * 4; // one warp's 32 x 16 FP32 output box
-constexpr int kOutBufs = 2;                // output staging boxes per epilogue warp, alternating
+constexpr int kOutBufs = 1;                // output staging boxes per epilogue warp
 constexpr int kOffH = 0;
 constexpr int kOffW = kOffH + kSlots * kHBytes;
 constexpr int kOffO = kOffW + kWStages * kWBytes;
@@ -124,16 +124,17 @@ __device__ __forceinline__ void epi_hidden(unsigned char* h_gen, int col, int tr
 }
 
 // Epilogue of 32 accumulator columns of the output layer (output columns gcol..): bias added, stored as
-// two 32-row x 16-column FP32 boxes through the warp's two alternating staging buffers (o_gen / o_sm,
-// generic and shared addresses); boxes wholly past n_out are neither staged nor stored, so that every
-// staged buffer has its store committed (the alternation relies on it). Returns the next buffer.
+// two 32-row x 16-column FP32 boxes through the warp's staging buffers (o_gen / o_sm, generic and
+// shared addresses; kOutBufs of them, in turn). Boxes wholly past n_out are neither staged nor
+// stored, so that every staged buffer has its store committed (the rotation relies on it).
+// Returns the next buffer.
 __device__ __forceinline__ int epi_output(const Params& p, unsigned char* o_gen, uint32_t o_sm, int obuf, int gcol,
                                            int row0, int lane, const uint32_t (&r)[32], const float4 (&b)[8]) {
 #pragma unroll
     for (int hb = 0; hb < 2; ++hb) {
         const int bcol = gcol + hb * kOutCols;
         if (bcol >= p.n_out) break;
-        // the staging buffer's previous store (two boxes back) has read it
+        // the staging buffer's previous store (kOutBufs boxes back) has read it
         if (lane == 0) bulk_wait_read<kOutBufs - 1>();
         __syncwarp();
         // 64-byte rows, 16-byte chunk q of row `lane` at chunk q ^ ((lane >> 1) & 3)
@@ -155,7 +156,7 @@ __device__ __forceinline__ int epi_output(const Params& p, unsigned char* o_gen,
             tma_store_2d(&p.y, o_sm + (uint32_t)obuf * kOutBox, bcol, row0);
             bulk_commit();
         }
-        obuf ^= 1;
+        obuf = obuf + 1 == kOutBufs ? 0 : obuf + 1;
     }
     return obuf;
 }
@@ -327,34 +328,21 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_kernel(const __grid_c
             if (!__all_sync(0xffffffffu, got && !*s_abort)) { ok = false; break; }
             tc::tc_fence_after();
             unsigned char* h_gen = gbase + kOffH + (size_t)s * kHBytes;
-            // 64 columns per round: both TMEM loads and the bias loads in flight before one wait
+            // 32 columns per round; the bias loads are issued with the TMEM load, before the wait
 #pragma unroll 1
-            for (int cc = 0; cc < cw; cc += 64) {
+            for (int cc = 0; cc < cw; cc += 32) {
                 const int col = group * cw + cc;  // column within the chunk
                 const int gcol = c * 256 + col;
                 if (!hidden_l && gcol >= p.n_out) continue;
-                const bool two = cw - cc > 32 && (hidden_l || gcol + 32 < p.n_out);  // warp-uniform
-                const uint32_t ta = taddr + lane_base + 256u * s + (uint32_t)col;
-                uint32_t ra[32], rb[32];
-                tc::tmem_ld32(ta, ra);
-                if (two) tc::tmem_ld32(ta + 32, rb);
+                uint32_t r[32];
+                tc::tmem_ld32(taddr + lane_base + 256u * s + (uint32_t)col, r);
                 const float4* b4 = reinterpret_cast<const float4*>(bias + gcol);
-                float4 ba[8], bb[8];
+                float4 bv[8];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) ba[q] = __ldg(&b4[q]);
-                if (two) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) bb[q] = __ldg(&b4[8 + q]);
-                }
+                for (int q = 0; q < 8; ++q) bv[q] = __ldg(&b4[q]);
                 tc::tmem_ld_wait();
-                if (hidden_l) {
-                    epi_hidden(h_gen, col, trow, ra, ba);
-                    if (two) epi_hidden(h_gen, col + 32, trow, rb, bb);
-                } else {
-                    const int row0 = t * 128 + quarter * 32;
-                    obuf = epi_output(p, o_gen, o_sm, obuf, gcol, row0, lane, ra, ba);
-                    if (two) obuf = epi_output(p, o_gen, o_sm, obuf, gcol + 32, row0, lane, rb, bb);
-                }
+                if (hidden_l) epi_hidden(h_gen, col, trow, r, bv);
+                else obuf = epi_output(p, o_gen, o_sm, obuf, gcol, t * 128 + quarter * 32, lane, r, bv);
             }
             tc::tc_fence_before();
             if (hidden_l) fence_proxy_async();  // H writes before the next layer's MMAs read them

@@ -45,7 +45,7 @@ static void free_context(Context* c) {
     for (void* p : dbufs)
         if (p) cudaFree(p);
     void* hbufs[] = {c->h_cancel, c->h_absorb, c->h_det, c->h_tbin, c->h_ledger, c->h_status, c->h_maps,
-                     c->h_nz_offsets, c->h_nz_idx, c->h_nz_val};
+                     c->h_nz_offsets, c->h_nz_idx, c->h_nz_val, c->h_traj};
     for (void* p : hbufs)
         if (p) cudaFreeHost(p);
     for (cudaEvent_t& e : c->ev)
@@ -691,11 +691,13 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         XMC_CUDA(cudaMemcpyAsync(c->h_ledger + kLedgerSlots, c->d_replay_ledger, led_b, cudaMemcpyDeviceToHost, c->stream));
     XMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
     // maps: the scattering map through its pinned staging; the trajectory maps as the list of their
-    // non-zero cells (count pass and scan, the list's length to the host, write pass, copy)
+    // non-zero cells (count pass and scan, the list's length to the host, write pass, copy), or
+    // dense when the list (12 bytes per cell) would be larger than the maps (8 bytes per cell)
     unsigned long long* hs = c->h_maps;
     const size_t G = (size_t)c->grid_size;
     if (want_scat) XMC_CUDA(cudaMemcpyAsync(hs, c->d_scatter, absorb_b, cudaMemcpyDeviceToHost, c->stream));
     size_t nz_total = 0;
+    bool traj_sparse = true;
     std::vector<size_t> map_start;
     if (want_traj) {
         const size_t D = (size_t)c->n_dets;
@@ -717,7 +719,19 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         map_start.resize(D + 1);
         for (size_t d = 0; d < D; ++d) map_start[d] = (size_t)c->h_nz_offsets[d * bpm];
         map_start[D] = nz_total;
-        if (nz_total > c->nz_cap) {
+        const size_t dense_b = absorb_b * D;
+        traj_sparse = (sizeof(unsigned) + sizeof(unsigned long long)) * nz_total < dense_b;
+        if (!traj_sparse) {
+            if (c->h_traj_bytes < dense_b) {
+                if (c->h_traj) cudaFreeHost(c->h_traj);
+                c->h_traj = nullptr;
+                c->h_traj_bytes = 0;
+                XMC_CUDA(cudaHostAlloc((void**)&c->h_traj, dense_b, cudaHostAllocDefault));
+                c->h_traj_bytes = dense_b;
+            }
+            XMC_CUDA(cudaMemcpyAsync(c->h_traj, c->d_traj, dense_b, cudaMemcpyDeviceToHost, c->stream));
+        }
+        if (traj_sparse && nz_total > c->nz_cap) {
             const size_t cap = nz_total + nz_total / 4 + 1024;
             if (c->d_nz_idx) cudaFree(c->d_nz_idx);
             if (c->d_nz_val) cudaFree(c->d_nz_val);
@@ -728,7 +742,7 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
             XMC_CUDA(cudaMalloc(&c->d_nz_val, sizeof(unsigned long long) * cap));
             c->nz_cap = cap;
         }
-        if (nz_total > c->h_nz_cap) {
+        if (traj_sparse && nz_total > c->h_nz_cap) {
             const size_t cap = c->nz_cap;
             if (c->h_nz_idx) cudaFreeHost(c->h_nz_idx);
             if (c->h_nz_val) cudaFreeHost(c->h_nz_val);
@@ -739,9 +753,10 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
             XMC_CUDA(cudaHostAlloc((void**)&c->h_nz_val, sizeof(unsigned long long) * cap, cudaHostAllocDefault));
             c->h_nz_cap = cap;
         }
-        XMC_CUDA(sparse_maps_write((const unsigned long long*)c->d_traj, G, (int)D, c->d_nz_offsets, c->d_nz_idx,
-                                   c->d_nz_val, c->stream));
-        if (nz_total) {
+        if (traj_sparse)
+            XMC_CUDA(sparse_maps_write((const unsigned long long*)c->d_traj, G, (int)D, c->d_nz_offsets, c->d_nz_idx,
+                                       c->d_nz_val, c->stream));
+        if (traj_sparse && nz_total) {
             XMC_CUDA(cudaMemcpyAsync(c->h_nz_idx, c->d_nz_idx, sizeof(unsigned) * nz_total, cudaMemcpyDeviceToHost,
                                      c->stream));
             XMC_CUDA(cudaMemcpyAsync(c->h_nz_val, c->d_nz_val, sizeof(unsigned long long) * nz_total,
@@ -787,7 +802,22 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
             if (want_scat)
                 for (size_t i = a; i < b; ++i) out->scattering[i] += (double)hs[i] * inv_scale;
         });
-        if (want_traj && nz_total) {
+        if (want_traj && !traj_sparse) {
+            // dense copy: each thread a slice of the grid in every map, non-zero cells only
+            const unsigned hd = host_threads_for(G * (size_t)c->n_dets);
+            const size_t pd = (G + hd - 1) / hd;
+            parallel_parts(hd, [&](unsigned t) {
+                const size_t a = std::min(G, t * pd), b = std::min(G, a + pd);
+                for (int d = 0; d < c->n_dets; ++d) {
+                    DetectorInfo& D = out->detectorInfo[d];
+                    if (!D.trajectory || D.trajectorySize != c->grid_size) continue;
+                    const unsigned long long* src = c->h_traj + (size_t)d * G;
+                    for (size_t i = a; i < b; ++i)
+                        if (src[i]) D.trajectory[i] += src[i];
+                }
+            });
+        }
+        if (want_traj && traj_sparse && nz_total) {
             const unsigned hz = host_threads_for(nz_total);
             const size_t pz = (nz_total + hz - 1) / hz;
             parallel_parts(hz, [&](unsigned t) {
@@ -808,11 +838,12 @@ static int run(Context* c, uint64_t seed, uint64_t first, uint64_t n, OutputInfo
         led->total_ms = t_ms;
         led->h2d_bytes = c->h2d_bytes + sizeof(KParams);
         // every device-to-host copy of this call: tallies, ledgers and status, the scattering map, and
-        // the sparse trajectory maps (block offsets, then the (cell, count) pairs)
+        // the trajectory maps (block offsets, then the (cell, count) pairs or the dense maps)
         size_t maps_b = want_scat ? absorb_b : 0;
         if (want_traj)
             maps_b += sizeof(unsigned long long) * ((size_t)c->n_dets * sparse_blocks_per_map(G) + 1) +
-                      (sizeof(unsigned) + sizeof(unsigned long long)) * nz_total;
+                      (traj_sparse ? (sizeof(unsigned) + sizeof(unsigned long long)) * nz_total
+                                   : absorb_b * (size_t)c->n_dets);
         led->d2h_bytes = (out ? absorb_b + tbin_b : 0) + det_b + led_b + 16 + (traj ? led_b : 0) + maps_b;
         led->n_replay_mismatch = traj ? c->h_ledger[kLedgerSlots + L_N_REPLAY_MISMATCH] : 0;
         led->n_trajectory_replayed = traj ? c->last_replayed : 0;

@@ -221,6 +221,7 @@ struct Context {
     unsigned* d_nz_idx = nullptr; unsigned long long* d_nz_val = nullptr; size_t nz_cap = 0;
     unsigned long long* h_nz_offsets = nullptr;  // [maps x blocks per map + 1]: offsets, then the last count
     unsigned* h_nz_idx = nullptr; unsigned long long* h_nz_val = nullptr; size_t h_nz_cap = 0;
+    unsigned long long* h_traj = nullptr; size_t h_traj_bytes = 0;  // dense copy, when the list would be larger
     int* h_status = nullptr;
     uint64_t last_n = 0;
     double last_kernel_ms = 0.0, last_total_ms = 0.0;

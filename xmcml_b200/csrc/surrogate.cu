@@ -14,6 +14,7 @@
 // lanes of a warp hold 32 consecutive rows), and each Adam step refreshes W_l and W_l^T in BF16
 // from the FP32 master weights. Loss: mean squared error over rows x n_out.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -421,6 +422,7 @@ struct xmc_mlp {
     uint64_t g_seed = 0;
     float* h_y = nullptr;           // pinned staging of the outputs read back by xmc_mlp_forward (lazy)
     size_t h_y_floats = 0;
+    cudaEvent_t ev_chunk[8] = {};   // completion of each chunk of that read-back (lazy)
 };
 
 namespace xmc {
@@ -444,6 +446,8 @@ void free_mlp(xmc_mlp* m) {
     for (cudaEvent_t e : m->ev)
         if (e) cudaEventDestroy(e);
     if (m->h_y) cudaFreeHost(m->h_y);
+    for (cudaEvent_t e : m->ev_chunk)
+        if (e) cudaEventDestroy(e);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
 }
@@ -760,7 +764,9 @@ extern "C" int xmc_mlp_forward(xmc_mlp* m, const float* x, int rows, float* y, d
     if (st) return st;
     XM_CUDA(cudaEventRecord(m->ev[1], m->stream));
     // outputs through pinned staging (kept by the model, sized for its row capacity), then into the
-    // caller's array on up to 8 host threads
+    // caller's array on up to 8 host threads. Large outputs go back in 8 chunks of rows, each with
+    // its own event, and every thread copies its share of a chunk as soon as that chunk has landed,
+    // so the host copies overlap the device-to-host transfer of the later chunks.
     const size_t nf = (size_t)rows * m->spec.n_out;
     if (m->h_y_floats < nf) {
         if (m->h_y) cudaFreeHost(m->h_y);
@@ -769,13 +775,28 @@ extern "C" int xmc_mlp_forward(xmc_mlp* m, const float* x, int rows, float* y, d
         XM_CUDA(cudaHostAlloc((void**)&m->h_y, sizeof(float) * (size_t)m->cap * m->spec.n_out, cudaHostAllocDefault));
         m->h_y_floats = (size_t)m->cap * m->spec.n_out;
     }
-    XM_CUDA(cudaMemcpyAsync(m->h_y, m->y, sizeof(float) * nf, cudaMemcpyDeviceToHost, m->stream));
-    XM_CUDA(cudaStreamSynchronize(m->stream));
+    const int chunks = nf < ((size_t)1 << 22) ? 1 : 8;
+    const size_t cf = ((size_t)(rows + chunks - 1) / chunks) * m->spec.n_out;  // floats per chunk (whole rows)
+    for (int k = 0; k < chunks; ++k) {
+        if (!m->ev_chunk[k]) XM_CUDA(cudaEventCreateWithFlags(&m->ev_chunk[k], cudaEventDisableTiming));
+        const size_t a = std::min(nf, k * cf), b = std::min(nf, a + cf);
+        if (a < b)
+            XM_CUDA(cudaMemcpyAsync(m->h_y + a, m->y + a, sizeof(float) * (b - a), cudaMemcpyDeviceToHost, m->stream));
+        XM_CUDA(cudaEventRecord(m->ev_chunk[k], m->stream));
+    }
     const unsigned parts = nf < ((size_t)1 << 20) ? 1u : std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-    const size_t per = (nf + parts - 1) / parts;
+    std::atomic<int> copy_err{0};
     auto copy_part = [&](unsigned p) {
-        const size_t a = std::min(nf, p * per), b = std::min(nf, a + per);
-        if (a < b) std::memcpy(y + a, m->h_y + a, sizeof(float) * (b - a));
+        for (int k = 0; k < chunks; ++k) {
+            if (cudaEventSynchronize(m->ev_chunk[k]) != cudaSuccess) {
+                copy_err = 1;
+                return;
+            }
+            const size_t a = std::min(nf, k * cf), b = std::min(nf, a + cf);
+            const size_t per = (b - a + parts - 1) / parts;
+            const size_t pa = std::min(b, a + p * per), pb = std::min(b, pa + per);
+            if (pa < pb) std::memcpy(y + pa, m->h_y + pa, sizeof(float) * (pb - pa));
+        }
     };
     std::vector<std::thread> pool;
     unsigned started = 1;
@@ -786,6 +807,11 @@ extern "C" int xmc_mlp_forward(xmc_mlp* m, const float* x, int rows, float* y, d
     copy_part(0);
     for (unsigned p = started; p < parts; ++p) copy_part(p);
     for (auto& th : pool) th.join();
+    if (copy_err) {
+        const cudaError_t e = cudaStreamSynchronize(m->stream);
+        return mfail(XMC_ERR_DEVICE, std::string("reading the outputs back failed: ") +
+                                         cudaGetErrorString(e != cudaSuccess ? e : cudaErrorUnknown));
+    }
     float t = 0.0f;
     XM_CUDA(cudaEventElapsedTime(&t, m->ev[0], m->ev[1]));
     if (ms) *ms = t;

@@ -279,3 +279,28 @@ def test_no_cpu_fallback_without_gpu(tmp_path):
     with pytest.raises(_lib.XmcError) as e:
         api.Transport(m)
     assert e.value.status == S.XMC_ERR_DEVICE
+
+
+@pytest.mark.parametrize("grid", [16, 256])
+def test_bad_vertex_index_is_reported_before_the_gpu(tmp_path, grid):
+    """xmc_create checks every triangle's vertex indices while it gathers the mesh (on several host
+    threads for the 2 x 130,050-triangle mesh, on one for the small one) and reports the first bad
+    triangle in input order, before any device work, so this runs without a GPU."""
+    sc = scenes.height_field_tissue(photons=1000, grid=grid, time_bins=4)
+    xml, surf = sc.write(str(tmp_path), "bad")
+    m = api.Model(xml, surf)
+    s1, s0 = m.info.surface[1], m.info.surface[0]
+    late = s1.numberOfTriangles - 2
+    s1.triangles[late].z = -1
+    s1.triangles[5].y = s1.numberOfVertices + 3
+    lib = _lib.load()
+    o = S.XmcOptions()
+    lib.xmc_default_options(C.byref(o))
+    ctx = C.c_void_p()
+    assert lib.xmc_create(C.byref(m.info), C.byref(o), C.byref(ctx)) == S.XMC_ERR_INVALID_INPUT
+    assert _lib.last_error() == "surface 1 triangle 5: vertex index out of range"
+    s1.triangles[5].y = 0
+    assert lib.xmc_create(C.byref(m.info), C.byref(o), C.byref(ctx)) == S.XMC_ERR_INVALID_INPUT
+    assert _lib.last_error() == f"surface 1 triangle {late}: vertex index out of range"
+    assert s0.numberOfTriangles > 0
+    m.close()

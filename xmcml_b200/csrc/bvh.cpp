@@ -165,6 +165,11 @@ struct Builder {
     }
 };
 
+// host threads for a loop over n independent items: one below 65,536 items, else up to 16
+static unsigned host_parts(size_t n) {
+    return n < 65536 ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+}
+
 void pad_box(float lo[3], float hi[3]) {
     for (int k = 0; k < 3; ++k) {
         float m = 4e-7f * std::max(1.0f, std::max(std::fabs(lo[k]), std::fabs(hi[k])));
@@ -191,15 +196,23 @@ bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err, int g
     B.v.resize(9 * (size_t)ntri);
     B.surf.resize(ntri);
     B.cen.resize(3 * (size_t)ntri);
-    for (int s = 0, t = 0; s < in->numberOfSurfaces; ++s) {
-        const Surface& S = in->surface[s];
-        for (int j = 0; j < S.numberOfTriangles; ++j, ++t) {
-            const xmc_ref_int3& T = S.triangles[j];
+    // FP32 vertices, centroids and surface ids, each host thread a range of triangles; a bad vertex
+    // index is reported for the first triangle (in input order) that has one
+    const unsigned parts = host_parts(ntri);
+    const size_t per = ((size_t)ntri + parts - 1) / parts;
+    std::vector<int> bad(parts, -1);
+    parallel_parts(parts, [&](unsigned part) {
+        const int t0 = (int)std::min((size_t)ntri, part * per), t1 = (int)std::min((size_t)ntri, (part + 1) * per);
+        int s = (int)(std::upper_bound(surf_base.begin(), surf_base.end() - 1, t0) - surf_base.begin()) - 1;
+        for (int t = t0; t < t1; ++t) {
+            while (t >= surf_base[s + 1]) ++s;
+            const Surface& S = in->surface[s];
+            const xmc_ref_int3& T = S.triangles[t - surf_base[s]];
             const int id[3] = {T.x, T.y, T.z};
             for (int c = 0; c < 3; ++c) {
                 if (id[c] < 0 || id[c] >= S.numberOfVertices) {
-                    *err = "surface " + std::to_string(s) + " triangle " + std::to_string(j) + ": vertex index out of range";
-                    return false;
+                    bad[part] = t;
+                    return;
                 }
                 const xmc_ref_double3& P = S.vertices[id[c]];
                 B.v[9 * (size_t)t + 3 * c + 0] = (float)P.x;
@@ -210,7 +223,15 @@ bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err, int g
                 B.cen[3 * (size_t)t + k] = (B.v[9 * (size_t)t + k] + B.v[9 * (size_t)t + 3 + k] + B.v[9 * (size_t)t + 6 + k]) / 3.0f;
             B.surf[t] = s;
         }
-    }
+    });
+    for (unsigned part = 0; part < parts; ++part)
+        if (bad[part] >= 0) {
+            const int t = bad[part];
+            const int s = (int)(std::upper_bound(surf_base.begin(), surf_base.end() - 1, t) - surf_base.begin()) - 1;
+            *err = "surface " + std::to_string(s) + " triangle " + std::to_string(t - surf_base[s]) +
+                   ": vertex index out of range";
+            return false;
+        }
     out->nodes.clear();
     out->tris.clear();
     out->n_nodes = out->n_tris = 0;
@@ -359,33 +380,43 @@ bool build_geometry(const InputInfo* in, GeomImage* out, std::string* err, int g
     out->nodes.assign(2 * (size_t)n, make_float4(0, 0, 0, 0));
     out->n_tris = ntri;
     out->tris.assign(3 * (size_t)ntri, make_float4(0, 0, 0, 0));
-    for (int x = 0; x < n; ++x) {
-        const BNode& N = B.nodes[x];
-        float lo[3] = {N.lo[0], N.lo[1], N.lo[2]}, hi[3] = {N.hi[0], N.hi[1], N.hi[2]};
-        pad_box(lo, hi);
-        int child;
-        if (N.count > 0) child = -1 - ((N.first << 3) | (N.count - 1));
-        else child = newid[N.left];
-        int i = newid[x];
-        out->nodes[2 * (size_t)i + 0] = make_float4(lo[0], lo[1], lo[2], __builtin_bit_cast(float, child));
-        out->nodes[2 * (size_t)i + 1] = make_float4(hi[0], hi[1], hi[2], __builtin_bit_cast(float, miss[x]));
-    }
-    for (int i = 0; i < ntri; ++i) {
-        int t = B.order[i];
-        const float* p = &B.v[9 * (size_t)t];
-        out->tris[3 * (size_t)i + 0] = make_float4(p[0], p[1], p[2], __builtin_bit_cast(float, B.surf[t]));
-        out->tris[3 * (size_t)i + 1] = make_float4(p[3], p[4], p[5], __builtin_bit_cast(float, t));
-        float emin = INFINITY;
-        for (int e = 0; e < 3; ++e) {
-            const float* A = p + 3 * e;
-            const float* Bv = p + 3 * ((e + 1) % 3);
-            const float dx = Bv[0] - A[0], dy = Bv[1] - A[1], dz = Bv[2] - A[2];
-            emin = std::min(emin, std::sqrt(dx * dx + dy * dy + dz * dz));
+    // nodes and triangles in their device layout, each host thread a range (every output slot is
+    // written by exactly one thread)
+    const unsigned nparts = host_parts(n);
+    const size_t nper = ((size_t)n + nparts - 1) / nparts;
+    parallel_parts(nparts, [&](unsigned part) {
+        const int x1 = (int)std::min((size_t)n, (part + 1) * nper);
+        for (int x = (int)std::min((size_t)n, part * nper); x < x1; ++x) {
+            const BNode& N = B.nodes[x];
+            float lo[3] = {N.lo[0], N.lo[1], N.lo[2]}, hi[3] = {N.hi[0], N.hi[1], N.hi[2]};
+            pad_box(lo, hi);
+            int child;
+            if (N.count > 0) child = -1 - ((N.first << 3) | (N.count - 1));
+            else child = newid[N.left];
+            int i = newid[x];
+            out->nodes[2 * (size_t)i + 0] = make_float4(lo[0], lo[1], lo[2], __builtin_bit_cast(float, child));
+            out->nodes[2 * (size_t)i + 1] = make_float4(hi[0], hi[1], hi[2], __builtin_bit_cast(float, miss[x]));
         }
-        float band = emin > 0.0f ? kEdgeBandLength / emin : kEdgeBandMax;
-        band = std::min(kEdgeBandMax, std::max(kEdgeBandMin, band));
-        out->tris[3 * (size_t)i + 2] = make_float4(p[6], p[7], p[8], band);
-    }
+    });
+    parallel_parts(parts, [&](unsigned part) {
+        const int i1 = (int)std::min((size_t)ntri, (part + 1) * per);
+        for (int i = (int)std::min((size_t)ntri, part * per); i < i1; ++i) {
+            int t = B.order[i];
+            const float* p = &B.v[9 * (size_t)t];
+            out->tris[3 * (size_t)i + 0] = make_float4(p[0], p[1], p[2], __builtin_bit_cast(float, B.surf[t]));
+            out->tris[3 * (size_t)i + 1] = make_float4(p[3], p[4], p[5], __builtin_bit_cast(float, t));
+            float emin = INFINITY;
+            for (int e = 0; e < 3; ++e) {
+                const float* A = p + 3 * e;
+                const float* Bv = p + 3 * ((e + 1) % 3);
+                const float dx = Bv[0] - A[0], dy = Bv[1] - A[1], dz = Bv[2] - A[2];
+                emin = std::min(emin, std::sqrt(dx * dx + dy * dy + dz * dz));
+            }
+            float band = emin > 0.0f ? kEdgeBandLength / emin : kEdgeBandMax;
+            band = std::min(kEdgeBandMax, std::max(kEdgeBandMin, band));
+            out->tris[3 * (size_t)i + 2] = make_float4(p[6], p[7], p[8], band);
+        }
+    });
     return true;
 }
 
@@ -582,48 +613,54 @@ void build_xy_grid(const GeomImage& g, GridImage* out, int tris_per_cell) {
     // one interval and the intervals are disjoint and ordered); cell_runs keeps their counts.
     out->cell_z.assign(2 * nc, make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY));
     out->cell_runs.assign(nc, 0u);
-    std::vector<std::pair<float, float>> iv;
-    for (size_t c = 0; c < nc; ++c) {
-        float4* ce = out->entries.data() + out->cells[c].x;
-        const unsigned int cn = out->cells[c].y;
-        std::sort(ce, ce + cn, [](const float4& a, const float4& b) {
-            if (a.x != b.x) return a.x < b.x;
-            int ta, tb;
-            std::memcpy(&ta, &a.z, sizeof(ta));
-            std::memcpy(&tb, &b.z, sizeof(tb));
-            return ta < tb;
-        });
-        iv.clear();
-        for (unsigned int k = 0; k < cn; ++k) iv.push_back({ce[k].x, ce[k].y});
-        std::sort(iv.begin(), iv.end());
-        std::vector<std::pair<float, float>> m;
-        for (auto& v : iv) {
-            if (!m.empty() && v.first <= m.back().second) m.back().second = std::max(m.back().second, v.second);
-            else m.push_back(v);
+    // cells are independent: up to 16 host threads, each a contiguous range of cells
+    const unsigned parts = nc < 4096 ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t per = (nc + parts - 1) / parts;
+    parallel_parts(parts, [&](unsigned part) {
+        std::vector<std::pair<float, float>> iv, m;
+        const size_t c_end = std::min(nc, (part + 1) * per);
+        for (size_t c = part * per; c < c_end; ++c) {
+            float4* ce = out->entries.data() + out->cells[c].x;
+            const unsigned int cn = out->cells[c].y;
+            std::sort(ce, ce + cn, [](const float4& a, const float4& b) {
+                if (a.x != b.x) return a.x < b.x;
+                int ta, tb;
+                std::memcpy(&ta, &a.z, sizeof(ta));
+                std::memcpy(&tb, &b.z, sizeof(tb));
+                return ta < tb;
+            });
+            iv.clear();
+            for (unsigned int k = 0; k < cn; ++k) iv.push_back({ce[k].x, ce[k].y});
+            std::sort(iv.begin(), iv.end());
+            m.clear();
+            for (auto& v : iv) {
+                if (!m.empty() && v.first <= m.back().second) m.back().second = std::max(m.back().second, v.second);
+                else m.push_back(v);
+            }
+            while (m.size() > 4) {
+                size_t best = 0;
+                float gap = INFINITY;
+                for (size_t q = 0; q + 1 < m.size(); ++q)
+                    if (m[q + 1].first - m[q].second < gap) { gap = m[q + 1].first - m[q].second; best = q; }
+                m[best].second = std::max(m[best].second, m[best + 1].second);
+                m.erase(m.begin() + best + 1);
+            }
+            float z[8] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
+            for (size_t q = 0; q < m.size(); ++q) { z[2 * q] = m[q].first; z[2 * q + 1] = m[q].second; }
+            out->cell_z[2 * c] = make_float4(z[0], z[1], z[2], z[3]);
+            out->cell_z[2 * c + 1] = make_float4(z[4], z[5], z[6], z[7]);
+            unsigned int cnt[4] = {0, 0, 0, 0};
+            bool split = true;
+            for (unsigned int k = 0; k < cn; ++k) {
+                size_t q = 0;
+                while (q + 1 < m.size() && ce[k].x > m[q].second) ++q;
+                if (!(ce[k].x >= m[q].first && ce[k].y <= m[q].second)) split = false;  // not inside one interval
+                ++cnt[q];
+            }
+            for (int q = 0; q < 4; ++q) split = split && cnt[q] <= 255u;
+            out->cell_runs[c] = split ? (cnt[0] | cnt[1] << 8 | cnt[2] << 16 | cnt[3] << 24) : 0xffffffffu;
         }
-        while (m.size() > 4) {
-            size_t best = 0;
-            float gap = INFINITY;
-            for (size_t q = 0; q + 1 < m.size(); ++q)
-                if (m[q + 1].first - m[q].second < gap) { gap = m[q + 1].first - m[q].second; best = q; }
-            m[best].second = std::max(m[best].second, m[best + 1].second);
-            m.erase(m.begin() + best + 1);
-        }
-        float z[8] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
-        for (size_t q = 0; q < m.size(); ++q) { z[2 * q] = m[q].first; z[2 * q + 1] = m[q].second; }
-        out->cell_z[2 * c] = make_float4(z[0], z[1], z[2], z[3]);
-        out->cell_z[2 * c + 1] = make_float4(z[4], z[5], z[6], z[7]);
-        unsigned int cnt[4] = {0, 0, 0, 0};
-        bool split = true;
-        for (unsigned int k = 0; k < cn; ++k) {
-            size_t q = 0;
-            while (q + 1 < m.size() && ce[k].x > m[q].second) ++q;
-            if (!(ce[k].x >= m[q].first && ce[k].y <= m[q].second)) split = false;  // not inside one interval
-            ++cnt[q];
-        }
-        for (int q = 0; q < 4; ++q) split = split && cnt[q] <= 255u;
-        out->cell_runs[c] = split ? (cnt[0] | cnt[1] << 8 | cnt[2] << 16 | cnt[3] << 24) : 0xffffffffu;
-    }
+    });
 }
 
 // GenerateBVHTree replacement (mcml_intersection.cpp:316-344): a binned-SAH tree of this library

@@ -55,22 +55,6 @@ static void free_context(Context* c) {
     delete c;
 }
 
-// Runs body(t) for t in [0, parts) on up to `parts` host threads, the calling thread included. When
-// the system cannot start a thread (std::system_error), the parts that got no thread run on the
-// calling thread, so no C++ exception crosses the C-ABI.
-template <typename F>
-static void parallel_parts(unsigned parts, F body) {
-    std::vector<std::thread> pool;
-    unsigned started = 1;
-    try {
-        for (; started < parts; ++started) pool.emplace_back(body, started);
-    } catch (...) {
-    }
-    body(0);
-    for (unsigned t = started; t < parts; ++t) body(t);
-    for (auto& th : pool) th.join();
-}
-
 static unsigned host_threads_for(size_t n) {
     return n < ((size_t)1 << 18) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
 }
@@ -315,8 +299,13 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.smem_next = smem_next;
     kp.n_nodes = geom.n_nodes;
     kp.n_tris = geom.n_tris;
-    kp.n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
-    build_xy_grid(geom, &img->grid, opt.grid_cell_tris > 0 ? opt.grid_cell_tris : 8);
+    // the occupied z-slabs and the xy grid read only the geometry: built side by side
+    int n_zocc = 0;
+    parallel_parts(2, [&](unsigned t) {
+        if (t == 1) n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
+        else build_xy_grid(geom, &img->grid, opt.grid_cell_tris > 0 ? opt.grid_cell_tris : 8);
+    });
+    kp.n_zocc = n_zocc;
     kp.grid_x0 = img->grid.x0;
     kp.grid_y0 = img->grid.y0;
     kp.grid_icx = img->grid.icx;

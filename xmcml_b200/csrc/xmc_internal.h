@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -16,6 +17,22 @@
 #undef int3
 
 namespace xmc {
+
+// Runs body(t) for t in [0, parts) on up to `parts` host threads, the calling thread included. When
+// the system cannot start a thread (std::system_error), the parts that got no thread run on the
+// calling thread, so no C++ exception crosses the C-ABI.
+template <typename F>
+inline void parallel_parts(unsigned parts, F body) {
+    std::vector<std::thread> pool;
+    unsigned started = 1;
+    try {
+        for (; started < parts; ++started) pool.emplace_back(body, started);
+    } catch (...) {
+    }
+    body(0);
+    for (unsigned t = started; t < parts; ++t) body(t);
+    for (auto& th : pool) th.join();
+}
 
 // Fixed point of photon weights and tallies: weight 1.0 == 2^31.
 constexpr double kWeightScale = 2147483648.0;

@@ -18,14 +18,17 @@ constexpr int kNzThreads = 256;
 constexpr int kNzPerThread = 16;
 constexpr int kNzCells = kNzThreads * kNzPerThread;  // cells per block
 
-// Non-zero cells of block (blockIdx.x) of map (blockIdx.y); thread t reads cells t, t + 256, ...
+// Non-zero cells of one block of 4,096 cells: launch block b is block b % blocks_per_map of map
+// b / blocks_per_map (a 1-D grid, so the number of maps is not bound by the grid's y extent); thread t
+// reads cells t, t + 256, ...
 __global__ void __launch_bounds__(kNzThreads) nz_count_kernel(const unsigned long long* __restrict__ maps,
                                                               unsigned long long cells, unsigned blocks_per_map,
                                                               unsigned long long* __restrict__ counts) {
     using BlockReduce = cub::BlockReduce<unsigned, kNzThreads>;
     __shared__ typename BlockReduce::TempStorage tmp;
-    const unsigned long long base = (unsigned long long)blockIdx.x * kNzCells;
-    const unsigned long long* m = maps + (unsigned long long)blockIdx.y * cells;
+    const unsigned map = blockIdx.x / blocks_per_map, blk = blockIdx.x % blocks_per_map;
+    const unsigned long long base = (unsigned long long)blk * kNzCells;
+    const unsigned long long* m = maps + (unsigned long long)map * cells;
     unsigned cnt = 0;
 #pragma unroll
     for (int j = 0; j < kNzPerThread; ++j) {
@@ -33,7 +36,7 @@ __global__ void __launch_bounds__(kNzThreads) nz_count_kernel(const unsigned lon
         if (cell < cells && m[cell]) ++cnt;
     }
     const unsigned total = BlockReduce(tmp).Sum(cnt);
-    if (threadIdx.x == 0) counts[(size_t)blockIdx.y * blocks_per_map + blockIdx.x] = total;
+    if (threadIdx.x == 0) counts[blockIdx.x] = total;
 }
 
 // The same cells again: each thread writes its non-zero cells at the block's offset plus the count of
@@ -45,8 +48,9 @@ __global__ void __launch_bounds__(kNzThreads) nz_write_kernel(const unsigned lon
                                                               unsigned long long* __restrict__ val) {
     using BlockScan = cub::BlockScan<unsigned, kNzThreads>;
     __shared__ typename BlockScan::TempStorage tmp;
-    const unsigned long long base = (unsigned long long)blockIdx.x * kNzCells;
-    const unsigned long long* m = maps + (unsigned long long)blockIdx.y * cells;
+    const unsigned map = blockIdx.x / blocks_per_map, blk = blockIdx.x % blocks_per_map;
+    const unsigned long long base = (unsigned long long)blk * kNzCells;
+    const unsigned long long* m = maps + (unsigned long long)map * cells;
     unsigned long long v[kNzPerThread];
     unsigned cnt = 0;
 #pragma unroll
@@ -57,7 +61,7 @@ __global__ void __launch_bounds__(kNzThreads) nz_write_kernel(const unsigned lon
     }
     unsigned before = 0;
     BlockScan(tmp).ExclusiveSum(cnt, before);
-    unsigned long long o = offsets[(size_t)blockIdx.y * blocks_per_map + blockIdx.x] + before;
+    unsigned long long o = offsets[blockIdx.x] + before;
 #pragma unroll
     for (int j = 0; j < kNzPerThread; ++j) {
         if (v[j]) {
@@ -77,7 +81,8 @@ cudaError_t sparse_maps_count(const unsigned long long* maps, size_t cells, int 
     const unsigned bpm = sparse_blocks_per_map(cells);
     const size_t n = (size_t)bpm * n_maps;
     if (n == 0) return cudaSuccess;
-    nz_count_kernel<<<dim3(bpm, n_maps), kNzThreads, 0, st>>>(maps, cells, bpm, counts);
+    if (n > 0x7fffffffu) return cudaErrorInvalidValue;  // the 1-D grid's limit (beyond any map memory)
+    nz_count_kernel<<<(unsigned)n, kNzThreads, 0, st>>>(maps, cells, bpm, counts);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     size_t need = 0;
@@ -97,8 +102,10 @@ cudaError_t sparse_maps_count(const unsigned long long* maps, size_t cells, int 
 cudaError_t sparse_maps_write(const unsigned long long* maps, size_t cells, int n_maps, const unsigned long long* offsets,
                               unsigned* idx, unsigned long long* val, cudaStream_t st) {
     const unsigned bpm = sparse_blocks_per_map(cells);
-    if ((size_t)bpm * n_maps == 0) return cudaSuccess;
-    nz_write_kernel<<<dim3(bpm, n_maps), kNzThreads, 0, st>>>(maps, cells, bpm, offsets, idx, val);
+    const size_t n = (size_t)bpm * n_maps;
+    if (n == 0) return cudaSuccess;
+    if (n > 0x7fffffffu) return cudaErrorInvalidValue;
+    nz_write_kernel<<<(unsigned)n, kNzThreads, 0, st>>>(maps, cells, bpm, offsets, idx, val);
     return cudaGetLastError();
 }
 

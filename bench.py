@@ -63,7 +63,7 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-surrogate", action="store_true")
-    p.add_argument("--extra-workloads", default="planar,ellipsoid",
+    p.add_argument("--extra-workloads", default="planar,ellipsoid,batch",
                    help="workloads measured beside the headline one (comma list, '' for none)")
     p.add_argument("--extra-steps", type=int, default=3)
     p.add_argument("--no-roulette-variant", action="store_true")
@@ -420,6 +420,13 @@ def batch_config(args, inst):
 
 
 def run_batch_workload(args, rank, world, local, dist, torch, barrier):
+    """`--workload batch`: the batched sweep's line on its own (measure_batch)."""
+    line = measure_batch(args, rank, world, local, dist, torch, barrier, args.steps, args.warmup, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_batch(args, rank, world, local, dist, torch, barrier, n_steps, n_warmup, cpu_seconds):
     """Batched sweep: `instances` 3-layer planar instances (the sweep's distributions, photon budgets
     log-uniform in [1e5, 1e7] x budget_scale) in one persistent launch per step, replayed from a
     CUDA graph, launch shape from the autotuner. value: photons / device time of the transport
@@ -433,13 +440,13 @@ def run_batch_workload(args, rank, world, local, dist, torch, barrier):
     total = int(inst.photons.sum())
     b = XB.Batch(max_instances=K, device=local)
     tune = b.autotune(inst.subset(np.arange(min(128, K))), photons_cap=20000)
-    for w in range(args.warmup):
+    for w in range(n_warmup):
         b.run(inst)
     barrier()
     kms, walls, steps = [], [], 0
     with ClockSampler(local) as clk:
         barrier()
-        for k in range(args.steps):
+        for k in range(n_steps):
             t0 = time.perf_counter()
             out = b.run(inst)
             walls.append(time.perf_counter() - t0)
@@ -450,16 +457,16 @@ def run_batch_workload(args, rank, world, local, dist, torch, barrier):
     dev = torch.device(f"cuda:{local}")
     ker_ms = replicas.max_over_ranks(sum(kms), dist, dev)
     wall_s = replicas.max_over_ranks(sum(walls), dist, dev)
-    value = world * args.steps * total / (ker_ms / 1e3)
+    value = world * n_steps * total / (ker_ms / 1e3)
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    t = ker_ms / args.steps / 1e3
+    t = ker_ms / n_steps / 1e3
     ops = steps * (48 + 45)
     peak = 148 * 128 * sm_mhz * 1e6
     rl = {"bound": "issue", "achieved": ops / t / 1e12, "peak": peak / 1e12, "unit": "TOP/s", "frac": ops / t / peak,
           "traffic": None, "model": {"ops_per_step": 93, "steps_per_photon": steps / total,
                                      "peak_source": "nominal 148 SMs x 128 lanes x median sampled SM clock"}}
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_seconds > 0 and not args.no_cpu_baseline:
         try:
             from oracle import bind as OB
             if OB.ref_available(fast=True):
@@ -467,29 +474,30 @@ def run_batch_workload(args, rank, world, local, dist, torch, barrier):
                 rates = []
                 for k in range(4):
                     xml, surf = XB.to_scene(inst, k).write(d, f"i{k}")
-                    r, n_cpu, secs = cpu_reference_rate(xml, surf, args.cpu_seconds / 4, os.cpu_count() or 1)
+                    r, n_cpu, secs = cpu_reference_rate(xml, surf, cpu_seconds / 4, os.cpu_count() or 1)
                     rates.append(r)
                 cpu = {"value": float(np.mean(rates)), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference",
                        "sample": "the reference's LaunchOMP on the first 4 instances as planar models, "
-                                 f"{args.cpu_seconds / 4:.0f} s each, mean rate (weight cut semantics)"}
+                                 f"{cpu_seconds / 4:.0f} s each, mean rate (weight cut semantics)"}
         except Exception as e:
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference", "sample": f"failed: {e}"}
     b.close()
     R, T = 50, 20
     line = {"metric": "photons/s (batched 3-layer instances)", "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ker_ms / args.steps, "higher_is_better": True,
+            "steps": n_steps, "warmup": n_warmup, "ms_per_step": ker_ms / n_steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": batch_config(args, inst),
             "arm": {"autotune": tune, "parallelism": f"replicas x{world} (disjoint instance sets)",
                     "l2": "instance table re-uploaded and 24.6 MB of tallies zeroed every step"},
             "clocks": clocks,
-            "e2e": {"value": world * args.steps * total / wall_s, "unit": UNIT,
+            "e2e": {"value": world * n_steps * total / wall_s, "unit": UNIT,
                     "h2d_bytes_per_step": K * (32 + 5 * 48), "d2h_bytes_per_step": K * (R * T * 8 + R * 8 + 16 * 8) + 4,
                     "via": "xmc_batch_run with host instance table and host result arrays"},
-            "gpu_launches": 2 * args.steps, "roofline": rl, "cpu_baseline": cpu,
+            "gpu_launches": 2 * n_steps, "roofline": rl, "cpu_baseline": cpu,
             "walk": {"steps_per_photon": steps / total}}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    if cpu and cpu.get("value"):
+        cpu["gpu_value_over_cpu"] = value / cpu["value"]
+    return line
 
 
 def main():
@@ -530,12 +538,15 @@ def main():
                              local, dist, torch, barrier, atom, cpu_seconds=args.cpu_seconds)
     if not args.no_roulette_variant:
         # the same scene with roulette 1e-4 / 0.1 and no maps (the sweep's semantics), device time only
-        line["roulette_variant"] = measure_transport(args, args.workload, args.photons, args.extra_steps, 2, 0, rank,
+        line["roulette_variant"] = measure_transport(args, args.workload, args.photons, args.extra_steps, 3, 0, rank,
                                                      world, local, dist, torch, barrier, atom, roulette=True,
                                                      cpu_seconds=0)
     extra = {}
     for wl in [w for w in args.extra_workloads.split(",") if w and w != args.workload]:
-        extra[wl] = measure_transport(args, wl, args.photons, args.extra_steps, 2, min(args.e2e_steps, 2), rank, world,
+        if wl == "batch":  # the batched sweep at its own config: 3 warm-up and 2 timed steps of ~14 s
+            extra[wl] = measure_batch(args, rank, world, local, dist, torch, barrier, 2, 3, args.cpu_seconds)
+            continue
+        extra[wl] = measure_transport(args, wl, args.photons, args.extra_steps, 3, min(args.e2e_steps, 2), rank, world,
                                       local, dist, torch, barrier, atom, cpu_seconds=args.cpu_seconds * 0.75)
     if extra:
         line["workloads"] = extra
@@ -547,7 +558,8 @@ def main():
     line["gpu_launches"] = line["gpu_launches"] + sum(v["gpu_launches"] for v in extra.values()) + (
         line["roulette_variant"]["gpu_launches"] if "roulette_variant" in line else 0)
     line["gpu_launches_note"] = ("transport kernel launches (run pass + trajectory replay pass per call) of the timed "
-                                 "steps of the headline, the roulette variant and the extra workloads")
+                                 "steps of the headline, the roulette variant and the extra workloads, and the batched "
+                                 "sweep's kernel and reduction per timed step")
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -238,9 +238,9 @@ typedef struct xmc_options {
                                     * (0 = 4096, at most 65536; -1 = no log, every detected photon
                                     * is replayed)                                                 */
     int32_t  query_batch;          /* cooperative ray queries: rays a warp collects (the lanes that
-                                    * need one wait) before it runs a query round (0 = 8; 1 = every
+                                    * need one wait) before it runs a query round (0 = 12; 1 = every
                                     * iteration). A scheduling choice: tallies are the same bit for bit */
-    int32_t  grid_cell_tris;       /* triangles per cell the xy grid of short ray queries aims at (0 = 8;
+    int32_t  grid_cell_tris;       /* triangles per cell the xy grid of short ray queries aims at (0 = 12;
                                     * larger: coarser cells, fewer queries fall back to the BVH). A
                                     * speed choice: tallies are the same bit for bit              */
     int32_t  reserved[4];
@@ -328,9 +328,9 @@ int xmc_destroy(xmc_context* ctx);
 /* No counterpart in the reference (the project's autotuner of the transport kernel's launch shape).
  * Builds the device image of `input` under `base` (its flags, device and semantics are kept) and
  * times `sample_photons` photons (0 = 1e6) under every candidate: xy-grid density grid_cell_tris
- * {2, 8, 32} triangles per cell, block size {256, 512} at the occupancy maximum, photon ids a warp
+ * {2, 8, 16, 32} triangles per cell, block size {256, 512} at the occupancy maximum, photon ids a warp
  * claims from the dispenser at a time {32, 64}, and the ray-query scheme (warp-cooperative with
- * query_batch {1, 8, 16}, or lane by lane with XMC_LANE_QUERIES): 48 candidates, each timed once, the
+ * query_batch {1, 8, 12, 16}, or lane by lane with XMC_LANE_QUERIES): 80 candidates, each timed once, the
  * four fastest twice more on other photons. *best gets `base` with the fastest one, *best_ms (may be
  * NULL) its best kernel time. Every candidate gives bit-identical
  * tallies: a photon's random numbers, its candidate triangles' arithmetic and the choice among equal

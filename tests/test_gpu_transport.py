@@ -196,7 +196,7 @@ def test_cooperative_and_lane_queries_are_identical(tmp_path, which):
     m = api.Model(xml, surf)
     res = []
     for kw in (dict(), dict(lane_queries=True), dict(query_batch=8), dict(query_batch=16, grid_cell_tris=32),
-               dict(lane_queries=True, grid_cell_tris=8)):
+               dict(lane_queries=True, grid_cell_tris=8), dict(query_batch=12, grid_cell_tris=16)):
         t = api.Transport(m, roulette=True, scattering=True, trajectories=which == "heightfield", **kw)
         led = t.run(n, seed=17)
         res.append((t.tallies(), t.maps(), led))
@@ -608,7 +608,7 @@ def test_autotune_picks_a_shape_with_identical_tallies(tmp_path):
     m = api.Model(xml, surf)
     best, ms = api.autotune(m, sample_photons=20_000, roulette=True)
     assert ms > 0 and best.block_size in (256, 512) and best.photons_per_chunk in (32, 64)
-    assert best.query_batch in (1, 8, 16) and best.grid_cell_tris in (2, 8, 32)
+    assert best.query_batch in (1, 8, 12, 16) and best.grid_cell_tris in (2, 8, 16, 32)
     assert best.flags & S.XMC_ROULETTE
     res = []
     for opts in (api.options(roulette=True), best):

@@ -303,7 +303,7 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     int n_zocc = 0;
     parallel_parts(2, [&](unsigned t) {
         if (t == 1) n_zocc = occupied_z_slabs(geom, kp.zocc_lo, kp.zocc_hi);
-        else build_xy_grid(geom, &img->grid, opt.grid_cell_tris > 0 ? opt.grid_cell_tris : 8);
+        else build_xy_grid(geom, &img->grid, opt.grid_cell_tris > 0 ? opt.grid_cell_tris : 12);
     });
     kp.n_zocc = n_zocc;
     kp.grid_x0 = img->grid.x0;
@@ -314,7 +314,7 @@ int prepare_image(const InputInfo* in, const xmc_options* opt_in, HostImage* img
     kp.grid_ny = img->grid.ny;
     kp.n_big = (int)(img->grid.big.size() / 4);
     kp.coop_query = (opt.flags & XMC_LANE_QUERIES) ? 0 : 1;
-    kp.query_batch = opt.query_batch > 0 ? std::min(32, (int)opt.query_batch) : 8;
+    kp.query_batch = opt.query_batch > 0 ? std::min(32, (int)opt.query_batch) : 12;
     const int block = opt.block_size > 0 ? opt.block_size : 512;
     img->smem_bytes = smem_layout(nd, smem_nodes, smem_tris, smem_next, kp.coop_query ? block / 32 : 0);
     // ---- biasing (mcml_kernel.cpp:325-440) ----
@@ -962,18 +962,19 @@ int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sampl
     set_error("");
     DeviceGuard device_guard;
     const uint64_t n = sample_photons ? sample_photons : 1000000ull;
-    const int densities[] = {2, 8, 32};
+    const int densities[] = {2, 8, 16, 32};
+    const int n_dens = (int)(sizeof(densities) / sizeof(densities[0]));
     const int blocks[] = {256, 512};
     const int chunks[] = {32, 64};
-    const int batches[] = {1, 8, 16};
+    const int batches[] = {1, 8, 12, 16};
     struct Cand {
         xmc_options opt;
         double ms;
     };
     std::vector<Cand> cands;
-    std::vector<HostImage> images(3);
+    std::vector<HostImage> images(n_dens);
     std::string last_err;
-    for (int di = 0; di < 3; ++di) {
+    for (int di = 0; di < n_dens; ++di) {
         // the xy grid's cell size is part of the device image: one image per density
         xmc_options o;
         xmc_default_options(&o);
@@ -1002,7 +1003,8 @@ int xmc_autotune(const InputInfo* input, const xmc_options* base, uint64_t sampl
     }
     // launch-shape fields only: the tally arithmetic stays the same
     auto shaped = [&](const xmc_options& c) {
-        const int di = c.grid_cell_tris == densities[0] ? 0 : c.grid_cell_tris == densities[1] ? 1 : 2;
+        int di = 0;
+        while (di + 1 < n_dens && densities[di] != c.grid_cell_tris) ++di;
         HostImage img = images[di];
         img.opt = c;
         img.kp.flags = c.flags;
